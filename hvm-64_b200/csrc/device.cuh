@@ -1,0 +1,665 @@
+// Device runtime of the B200 interaction-net reducer.
+//
+// Heap: one HBM arena of 16-byte nodes (two 8-byte port words), addressed by
+// byte offset, so a node's other half is `addr ^ 8` exactly as in the
+// reference (runtime/src/addr.rs:36-50).  Node 0 is reserved (the free-list
+// terminator and a scratch target for guarded accesses).
+//
+// Every heap access is a strong GPU-scope operation (ld/st.relaxed.gpu or an
+// atomic), so no SM reads a stale L1 copy of a word another SM changed.  A
+// freshly allocated node is filled with LOCK and fenced before its address
+// can escape; readers treat LOCK as "not ready yet" and wait, which is the
+// reference's own protocol (runtime/src/wire.rs:67-75).
+//
+// Every wait is bounded: after `spin_limit` polls, or when another lane has
+// already failed, the wait gives up, the run's error word is set and all
+// warps drain and exit.  Every heap address is bounds-checked; an address
+// outside the arena sets HVM64_ERR_BAD_ADDR and is redirected to node 0, so a
+// protocol fault can never become a memory fault.
+#pragma once
+#include <stdint.h>
+
+#include "host.hpp"
+#include "hvm64.h"
+#include "num.h"
+
+namespace hvm {
+namespace dev {
+
+typedef unsigned long long ull;
+
+constexpr int WARPS = 8;            // warps per reducer block
+constexpr int THREADS = WARPS * 32;
+constexpr int SCAP = 256;           // per-warp shared-memory redex stack (power of two)
+constexpr int LBCAP = 8;            // per-lane buffer of redexes made by one interaction
+constexpr int CHUNK = 32;           // redexes per global-queue slot
+
+constexpr ull P_ERA = 2;
+constexpr ull P_FREE = 0x8000000000000000ull;
+constexpr ull P_LOCK = 0xFFFFFFFFFFFFFFF0ull;
+constexpr ull P_GONE = 0xFFFFFFFFFFFFFFFFull;
+constexpr ull A_MASK = 0x0000FFFFFFFFFFF8ull;
+constexpr ull X_BIT = 1ull << 47;  // expansion-agent Ref ports
+
+enum : int { RW_ANNI = 0, RW_COMM, RW_ERAS, RW_DREF, RW_OPER };
+
+// Global control block.  Hot counters sit on their own 128-byte lines.
+struct Ctrl {
+  ull bump;        // next never-used node index
+  ull heap_nodes;
+  ull heap_bytes;
+  ull chunk_nodes;
+  ull spin_limit;
+  ull deadline;    // %globaltimer ns
+  ull donate_min;
+  ull q_mask;
+  int error;
+  int error_net;
+  ull error_info;
+  ull pad0[6];
+  long long nets_left;
+  ull pad1[15];
+  long long hungry;
+  ull pad2[15];
+  ull q_head;
+  ull pad3[15];
+  ull q_tail;
+  ull pad4[15];
+  ull stat_donated, stat_spilled, stat_overflow, stat_taken;
+};
+
+struct NetState {  // 64 bytes
+  ull root;            // byte offset of the root wire
+  long long pending;   // warps holding this net's work + queued chunks
+  ull rw[5];
+  int prog;            // DevDef index of the boot program
+  int status;
+};
+
+struct Slot {  // 544 bytes: one chunk of up to 32 redexes of one net
+  ull seq;
+  unsigned net;
+  unsigned count;
+  ull pad[2];
+  ull r[2 * CHUNK];
+};
+
+struct Params {
+  ull* heap;
+  Ctrl* ctrl;
+  NetState* nets;
+  unsigned nnets;
+  Slot* q;
+  const DevDef* __restrict__ defs;
+  const DevInstr* __restrict__ instrs;
+  const ull* __restrict__ labbits;
+  unsigned ndefs;
+};
+
+// ---- strong memory operations --------------------------------------------
+__device__ __forceinline__ ull ld_gpu(const ull* p) {
+  ull v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_gpu(ull* p, ull v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ int ld_gpu32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ long long ld_gpu64s(const long long* p) {
+  return (long long)ld_gpu(reinterpret_cast<const ull*>(p));
+}
+__device__ __forceinline__ ull globaltimer() {
+  ull t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ---- ports (runtime/src/port.rs) ---------------------------------------------
+__device__ __forceinline__ unsigned ptag(ull p) { return unsigned(p & 7); }
+__device__ __forceinline__ unsigned plab(ull p) { return unsigned(p >> 48); }
+__device__ __forceinline__ ull paddr(ull p) { return p & A_MASK; }
+__device__ __forceinline__ ull mkport(unsigned tag, unsigned lab, ull addr) { return (ull(lab) << 48) | addr | tag; }
+__device__ __forceinline__ ull pvar(ull a) { return a | T_VAR; }
+__device__ __forceinline__ ull pred(ull a) { return a | T_RED; }
+__device__ __forceinline__ bool principal(ull p) { return ptag(p) >= T_REF; }
+__device__ __forceinline__ bool skippable(ull p) {  // port.rs:205-207
+  return ptag(p) == T_NUM || (ptag(p) == T_REF && plab(p) != 0xFFFF);
+}
+__device__ __forceinline__ bool is_expand(ull p) { return ptag(p) == T_REF && (p & X_BIT) != 0; }
+// Trg (runtime/src/linker.rs:228-281): a wire is its address with the Red tag.
+__device__ __forceinline__ bool trg_is_wire(ull t) { return ptag(t) == T_RED; }
+
+struct Lane {
+  const Params& P;
+  ull* H;
+  ull hb;
+  ull head;   // free-list head (byte address; 0 = empty)
+  ull bnext;  // bump chunk [bnext, bend) in node indices
+  ull bend;
+  ull rw[5];
+  unsigned net;
+  int pn;
+  ull pb[2 * LBCAP];
+
+  __device__ explicit Lane(const Params& p) : P(p), H(p.heap), hb(p.ctrl->heap_bytes), head(0), bnext(0), bend(0),
+                                              net(0), pn(0) {
+    for (int k = 0; k < 5; k++) rw[k] = 0;
+  }
+
+  __device__ void fail(int code, ull info) {
+    if (atomicCAS(&P.ctrl->error, 0, code) == 0) {
+      P.ctrl->error_info = info;
+      P.ctrl->error_net = int(net);
+    }
+  }
+  __device__ bool failed() const { return ld_gpu32(&P.ctrl->error) != 0; }
+
+  // One poll of a bounded wait; false = abandon the wait.
+  __device__ bool spin(unsigned& it) {
+    ++it;
+    if ((it & 63) == 0) {
+      if (failed()) return false;
+      if (it > P.ctrl->spin_limit) {
+        fail(HVM64_ERR_TIMEOUT, 0);
+        return false;
+      }
+      __nanosleep(64);
+    }
+    return true;
+  }
+
+  __device__ ull* at(ull a) {
+    if (a >= hb) {
+      fail(HVM64_ERR_BAD_ADDR, a);
+      a = 0;
+    }
+    return H + (a >> 3);
+  }
+  __device__ ull load(ull a) { return ld_gpu(at(a)); }
+  __device__ void store(ull a, ull v) { st_gpu(at(a), v); }
+  __device__ ull swap(ull a, ull v) { return atomicExch(at(a), v); }
+  __device__ ull cas(ull a, ull e, ull v) { return atomicCAS(at(a), e, v); }
+
+  // wire.rs:342-350
+  __device__ ull lock_target(ull w) {
+    unsigned it = 0;
+    for (;;) {
+      ull got = swap(w, P_LOCK);
+      if (got != P_LOCK) return got;
+      if (!spin(it)) return P_ERA;
+    }
+  }
+
+  // ---- allocator (runtime/src/allocator.rs:73-110) --------------------------
+  __device__ void half_free(ull a) {
+    store(a, P_FREE);
+    if (load(a ^ 8) == P_FREE) {
+      ull l = a & ~8ull;
+      if (cas(l, P_FREE, head) == P_FREE) head = l;
+    }
+  }
+  __device__ ull alloc() {
+    ull a;
+    if (head != 0) {
+      a = head;
+      head = load(a);
+    } else {
+      if (bnext == bend) {
+        ull n = P.ctrl->chunk_nodes;
+        ull s = atomicAdd(&P.ctrl->bump, n);
+        if (s + n > P.ctrl->heap_nodes) {
+          fail(HVM64_ERR_OOM, s);
+          return 0;
+        }
+        bnext = s;
+        bend = s + n;
+      }
+      a = (bnext++) << 4;
+    }
+    store(a, P_LOCK);
+    store(a ^ 8, P_LOCK);
+    __threadfence();  // LOCK is visible before the node's address escapes
+    return a;
+  }
+
+  // ---- redex pushes ----------------------------------------------------------
+  __device__ void overflow();
+  __device__ void push(ull a, ull b) {
+    if (pn == LBCAP) overflow();
+    pb[2 * pn] = a;
+    pb[2 * pn + 1] = b;
+    pn++;
+  }
+  // linker.rs:70-85
+  __device__ void redux(ull a, ull b) {
+    if (skippable(a) && skippable(b)) rw[RW_ERAS]++;
+    else push(a, b);
+  }
+
+  // ---- linker (runtime/src/linker.rs:25-203) --------------------------------
+  __device__ void half_link_port_port(ull a, ull b) {
+    if (ptag(a) == T_VAR) store(paddr(a), b);
+  }
+  __device__ void link_port_port(ull a, ull b) {
+    if (principal(a) && principal(b)) {
+      redux(a, b);
+    } else {
+      half_link_port_port(a, b);
+      half_link_port_port(b, a);
+    }
+  }
+  __device__ void link_wire_wire(ull aw, ull bw) {
+    ull ap = lock_target(aw);
+    ull bp = lock_target(bw);
+    if (principal(ap) && principal(bp)) {
+      half_free(aw);
+      half_free(bw);
+      redux(ap, bp);
+    } else {
+      half_link_wire_port(ap, aw, bp);
+      half_link_wire_port(bp, bw, ap);
+    }
+  }
+  __device__ void link_wire_port(ull aw, ull bp) {
+    ull ap = lock_target(aw);
+    if (principal(ap) && principal(bp)) {
+      half_free(aw);
+      redux(ap, bp);
+    } else {
+      half_link_wire_port(ap, aw, bp);
+      half_link_port_port(bp, ap);
+    }
+  }
+  __device__ void half_link_wire_port(ull ap, ull aw, ull bp) {
+    if (ptag(ap) == T_VAR) {
+      if (cas(paddr(ap), pvar(aw), bp) == pvar(aw)) {
+        half_free(aw);
+      } else if (ptag(bp) == T_VAR) {
+        store(aw, pred(paddr(bp)));
+      } else if (principal(bp)) {
+        store(aw, bp);
+        resolve_redirect_pri(ap, aw, bp);
+      } else {
+        fail(HVM64_ERR_BAD_PAIR, bp);
+      }
+    } else {
+      half_free(aw);
+    }
+  }
+  __device__ void resolve_redirect_pri(ull ap, ull aw, ull bp) {
+    unsigned it = 0;
+    for (;;) {
+      ull tw = paddr(ap);
+      ull tp = load(tw);
+      if (tp == P_LOCK) {
+        if (!spin(it)) return;
+        continue;
+      }
+      if (ptag(tp) == T_RED) {
+        half_free(tw);
+        ap = tp;
+        continue;
+      }
+      if (ptag(tp) == T_VAR) {
+        if (cas(tw, tp, bp) == tp) {
+          tw = paddr(tp);
+          tp = load(tw);
+          unsigned it2 = 0;
+          while (tp != P_LOCK && ptag(tp) == T_RED) {
+            half_free(tw);
+            tw = paddr(tp);
+            tp = load(tw);
+            if (!spin(it2)) return;
+          }
+          return;
+        }
+        if (!spin(it)) return;
+        continue;
+      }
+      if (principal(tp) || tp == P_GONE) {
+        ull xw = aw < tw ? aw : tw;
+        ull yw = aw < tw ? tw : aw;
+        ull xp = swap(xw, P_GONE);
+        if (xp != P_GONE) {
+          ull yp = swap(yw, P_GONE);
+          redux(xp, yp);
+        } else {
+          half_free(xw);
+          unsigned it3 = 0;
+          while (cas(yw, P_GONE, P_LOCK) != P_GONE)
+            if (!spin(it3)) return;
+          half_free(yw);
+        }
+        return;
+      }
+      fail(HVM64_ERR_BAD_PAIR, tp);
+      return;
+    }
+  }
+  __device__ void link_trg_port(ull a, ull b) {
+    if (trg_is_wire(a)) link_wire_port(a, b);
+    else link_port_port(a, b);
+  }
+  __device__ void link_trg(ull a, ull b) {
+    bool aw = trg_is_wire(a), bw = trg_is_wire(b);
+    if (aw && bw) link_wire_wire(a, b);
+    else if (aw) link_wire_port(a, b);
+    else if (bw) link_wire_port(b, a);
+    else link_port_port(a, b);
+  }
+  __device__ ull trg_target(ull t) { return trg_is_wire(t) ? load(t) : t; }
+  __device__ void free_trg(ull t) {
+    if (trg_is_wire(t)) half_free(t);
+  }
+
+  // ---- rules (runtime/src/interact.rs) ----------------------------------------
+  __device__ void anni2(ull a, ull b) {  // interact.rs:72-79
+    rw[RW_ANNI]++;
+    ull a1 = paddr(a), b1 = paddr(b);
+    link_wire_wire(a1, b1);
+    link_wire_wire(a1 ^ 8, b1 ^ 8);
+  }
+  __device__ void comm22(ull a, ull b) {  // interact.rs:118-141
+    rw[RW_COMM]++;
+    ull a1 = paddr(a), b1 = paddr(b);
+    ull A1 = alloc(), A2 = alloc(), B1 = alloc(), B2 = alloc();
+    unsigned ta = ptag(a), la = plab(a), tb = ptag(b), lb = plab(b);
+    link_port_port(pvar(A1), pvar(B1));
+    link_port_port(pvar(A1 ^ 8), pvar(B2));
+    link_port_port(pvar(A2), pvar(B1 ^ 8));
+    link_port_port(pvar(A2 ^ 8), pvar(B2 ^ 8));
+    link_wire_port(a1, mkport(tb, lb, B1));
+    link_wire_port(a1 ^ 8, mkport(tb, lb, B2));
+    link_wire_port(b1, mkport(ta, la, A1));
+    link_wire_port(b1 ^ 8, mkport(ta, la, A2));
+  }
+  __device__ void comm02(ull a, ull b) {  // interact.rs:162-168
+    rw[RW_COMM]++;
+    ull b1 = paddr(b);
+    link_wire_port(b1, a);
+    link_wire_port(b1 ^ 8, a);
+  }
+  __device__ void switch_num(ull a, ull b) {  // interact.rs:201-223
+    rw[RW_OPER]++;
+    ull a1 = paddr(a);
+    uint32_t num = uint32_t(b);
+    uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
+    if (n == 0) {
+      ull x = alloc();
+      link_port_port(pvar(x ^ 8), P_ERA);
+      link_wire_port(a1 ^ 8, pvar(x));
+      link_wire_port(a1, mkport(T_CTR, 0, x));
+    } else {
+      ull x = alloc(), y = alloc();
+      link_port_port(pvar(x), P_ERA);
+      link_port_port(pvar(x ^ 8), mkport(T_CTR, 0, y));
+      link_port_port(pvar(y), ull(num_u24(n - 1)));
+      link_wire_port(a1 ^ 8, pvar(y ^ 8));
+      link_wire_port(a1, mkport(T_CTR, 0, x));
+    }
+  }
+  __device__ uint32_t binary(uint32_t a, uint32_t op, uint32_t b) {
+    int e = 0;
+    uint32_t r = num_binary(a, op, b, &e);
+    if (e) fail(HVM64_ERR_DIV0, net);
+    return r;
+  }
+  __device__ void op_num(ull a, ull b) {  // interact.rs:251-270
+    uint32_t op = plab(a);
+    ull a1 = paddr(a);
+    ull t1 = load(a1);
+    if (ptag(t1) == T_NUM) {
+      rw[RW_OPER]++;
+      half_free(a1);
+      ull out = binary(uint32_t(b), op, uint32_t(t1));
+      link_wire_port(a1 ^ 8, out);
+    } else {
+      ull x = alloc();
+      link_port_port(pvar(x), ull(num_unary(op, uint32_t(b))));
+      link_wire_port(a1 ^ 8, pvar(x ^ 8));
+      link_wire_port(a1, mkport(T_OP, NT_SYM, x));
+    }
+  }
+
+  // def.rs:30-37 (LabSet::has); the expansion agent's set is LabSet::ALL.
+  __device__ bool def_has(ull ref, unsigned lab) {
+    if (ref & X_BIT) return lab < 0xFFFF;
+    unsigned id = unsigned((paddr(ref) >> 3) - 1);
+    if (id >= P.ndefs) {
+      fail(HVM64_ERR_BAD_INPUT, ref);
+      return true;
+    }
+    const DevDef& d = P.defs[id];
+    if (lab >= d.min_safe) return false;
+    unsigned w = lab >> 6;
+    if (w >= d.lab_len) return false;
+    return (P.labbits[d.lab_off + w] >> (lab & 63)) & 1;
+  }
+  // def.rs:177-189
+  __device__ void call(ull port, ull trg) {
+    if (ptag(trg) == T_CTR && !def_has(port, plab(trg))) return comm02(port, trg);
+    rw[RW_DREF]++;
+    if (port & X_BIT) expand_call(port, trg);
+    else run_def(unsigned((paddr(port) >> 3) - 1), trg);
+  }
+
+  // ---- interact.rs:6-44 --------------------------------------------------------
+  __device__ void interact(ull a, ull b) {
+    unsigned at = ptag(a), bt = ptag(b);
+    if (at <= T_VAR || bt <= T_VAR) return fail(HVM64_ERR_BAD_PAIR, a);
+    bool an = at == T_REF || at == T_NUM, bn = bt == T_REF || bt == T_NUM;
+    if (at == T_REF && bn && !skippable(a)) return call(a, b);
+    if (an && bt == T_REF && !skippable(b)) return call(b, a);
+    if (an && bn) {
+      rw[RW_ERAS]++;
+      return;
+    }
+    if (at == T_CTR && bt == T_SWITCH && plab(a) != 0) return comm22(a, b);
+    if (at == T_SWITCH && bt == T_CTR && plab(b) != 0) return comm22(a, b);
+    if ((at == T_CTR && bt == T_OP) || (at == T_OP && bt == T_CTR)) return comm22(a, b);
+    if (at == T_CTR && bt == T_CTR && plab(a) != plab(b)) return comm22(a, b);
+    if (at == bt && at >= T_OP) return anni2(a, b);
+    if (at == T_REF && bt == T_CTR && plab(b) >= plab(a)) return comm02(a, b);
+    if (at == T_CTR && bt == T_REF && plab(a) >= plab(b)) return comm02(b, a);
+    if (at == T_NUM && bt == T_CTR) return comm02(a, b);
+    if (at == T_CTR && bt == T_NUM) return comm02(b, a);
+    if (at == T_REF && a == P_ERA) return comm02(a, b);
+    if (bt == T_REF && b == P_ERA) return comm02(b, a);
+    if (at == T_REF) return call(a, b);
+    if (bt == T_REF) return call(b, a);
+    if (at == T_OP && bt == T_NUM) return op_num(a, b);
+    if (at == T_NUM && bt == T_OP) return op_num(b, a);
+    if (at == T_SWITCH && bt == T_NUM) return switch_num(a, b);
+    if (at == T_NUM && bt == T_SWITCH) return switch_num(b, a);
+    fail(HVM64_ERR_BAD_PAIR, a);
+  }
+
+  // ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) ----
+  __device__ void do_ctr(unsigned lab, ull trg, ull& o1, ull& o2) {
+    ull port = trg_target(trg);
+    if (ptag(port) == T_CTR && plab(port) == lab) {
+      free_trg(trg);
+      rw[RW_ANNI]++;
+      o1 = paddr(port);  // Trg::wire
+      o2 = paddr(port) ^ 8;
+      return;
+    }
+    ull n = alloc();
+    link_trg_port(trg, mkport(T_CTR, lab, n));
+    o1 = pvar(n);
+    o2 = pvar(n ^ 8);
+  }
+  __device__ void do_op(unsigned op, ull trg, ull& o1, ull& o2) {
+    ull port = trg_target(trg);
+    if (ptag(port) == T_NUM) {
+      free_trg(trg);
+      ull n = alloc();
+      store(n, ull(num_unary(op, uint32_t(port))));
+      o1 = mkport(T_OP, NT_SYM, n);
+      o2 = pvar(n ^ 8);
+      return;
+    }
+    if (port == P_ERA) {
+      free_trg(trg);
+      o1 = o2 = P_ERA;
+      return;
+    }
+    ull n = alloc();
+    link_trg_port(trg, mkport(T_OP, op, n));
+    o1 = pvar(n);
+    o2 = pvar(n ^ 8);
+  }
+  __device__ ull do_op_num(unsigned op, ull trg, uint32_t rhs) {
+    ull port = trg_target(trg);
+    if (ptag(port) == T_NUM) {
+      rw[RW_OPER]++;
+      free_trg(trg);
+      return ull(binary(uint32_t(port), op, rhs));
+    }
+    if (port == P_ERA) {
+      free_trg(trg);
+      return P_ERA;
+    }
+    ull n = alloc();
+    link_trg_port(trg, mkport(T_OP, op, n));
+    store(n, ull(rhs));
+    return pvar(n ^ 8);
+  }
+  __device__ ull create_wire_to(ull port) {  // node.rs:176-182
+    ull a = alloc();
+    half_free(a ^ 8);
+    link_port_port(port, pvar(a));
+    return a;
+  }
+  __device__ void do_switch(ull trg, ull& o1, ull& o2) {
+    ull port = trg_target(trg);
+    if (ptag(port) == T_NUM) {
+      rw[RW_OPER]++;
+      free_trg(trg);
+      uint32_t num = uint32_t(port);
+      uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
+      ull c1 = alloc();
+      if (n == 0) {
+        link_port_port(pvar(c1 ^ 8), P_ERA);
+        o1 = mkport(T_CTR, 0, c1);
+        o2 = create_wire_to(pvar(c1));
+      } else {
+        ull c2 = alloc();
+        link_port_port(pvar(c1), P_ERA);
+        link_port_port(pvar(c1 ^ 8), mkport(T_CTR, 0, c2));
+        link_port_port(pvar(c2), ull(num_u24(n - 1)));
+        o1 = mkport(T_CTR, 0, c1);
+        o2 = create_wire_to(pvar(c2 ^ 8));
+      }
+      return;
+    }
+    if (port == P_ERA) {
+      rw[RW_ERAS]++;
+      free_trg(trg);
+      o1 = o2 = P_ERA;
+      return;
+    }
+    ull m = alloc();
+    link_trg_port(trg, mkport(T_SWITCH, 0, m));
+    o1 = pvar(m);
+    o2 = pvar(m ^ 8);
+  }
+
+  __device__ void run_def(unsigned id, ull t0) {
+    if (id >= P.ndefs) return fail(HVM64_ERR_BAD_INPUT, id);
+    const DevDef d = P.defs[id];
+    ull R[MAX_REGS];
+    R[0] = t0;
+    const DevInstr* ins = P.instrs + d.ins_off;
+    for (unsigned k = 0; k < d.ins_len; k++) {
+      const DevInstr I = ins[k];
+      switch (I.k) {
+        case I_CONST: R[I.a] = I.port; break;
+        case I_LINK: link_trg(R[I.a], R[I.b]); break;
+        case I_LINKCONST: link_trg_port(R[I.a], I.port); break;
+        case I_CTR: {
+          ull x, y;
+          do_ctr(I.lab, R[I.a], x, y);
+          R[I.b] = x;
+          R[I.c] = y;
+          break;
+        }
+        case I_OP: {
+          ull x, y;
+          do_op(I.op, R[I.a], x, y);
+          R[I.b] = x;
+          R[I.c] = y;
+          break;
+        }
+        case I_OPNUM: R[I.c] = do_op_num(I.op, R[I.a], uint32_t(I.port)); break;
+        case I_SWITCH: {
+          ull x, y;
+          do_switch(R[I.a], x, y);
+          R[I.b] = x;
+          R[I.c] = y;
+          break;
+        }
+        case I_WIRES: {
+          ull a = alloc();
+          R[I.a] = pvar(a);
+          R[I.b] = a;
+          R[I.c] = pvar(a ^ 8);
+          R[I.d] = a ^ 8;
+          break;
+        }
+      }
+    }
+  }
+
+  // ---- expansion agent (runtime/src/net.rs:63-108) ----------------------------
+  // An agent is a Ref port with X_BIT whose address names a heap word holding
+  // its output port (the reference boxes an `ExpandDef { out }`).
+  __device__ ull new_expand(ull out) {
+    ull w = alloc();
+    half_free(w ^ 8);
+    store(w, out);
+    return mkport(T_REF, 0xFFFF, X_BIT | w);
+  }
+  __device__ ull take_expand(ull port) {
+    ull w = paddr(port) & ~X_BIT;
+    unsigned it = 0;
+    ull out;
+    while ((out = load(w)) == P_LOCK)
+      if (!spin(it)) break;
+    half_free(w);
+    return out;
+  }
+  __device__ void expand_call(ull self, ull port) {
+    if (ptag(port) == T_REF && port != P_ERA) {
+      if (port & X_BIT) {
+        ull a = take_expand(self), b = take_expand(port);
+        return link_port_port(a, b);
+      }
+      return call(port, self);
+    }
+    ull out = take_expand(self);
+    unsigned t = ptag(port);
+    if (t == T_RED) return fail(HVM64_ERR_BAD_PAIR, port);
+    if (t == T_REF || t == T_NUM || t == T_VAR) return link_port_port(out, port);
+    ull o1 = paddr(port);
+    ull n = alloc();
+    link_port_port(out, mkport(t, plab(port), n));
+    link_wire_port(o1, new_expand(pvar(n)));
+    link_wire_port(o1 ^ 8, new_expand(pvar(n ^ 8)));
+  }
+  // net.rs:65-69
+  __device__ ull expand(ull root) {
+    ull a = alloc();
+    half_free(a ^ 8);
+    link_wire_port(root, new_expand(pvar(a)));
+    return a;
+  }
+};
+
+}  // namespace dev
+}  // namespace hvm

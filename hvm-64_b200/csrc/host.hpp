@@ -1,0 +1,138 @@
+// Host side of the B200 reducer: the `.hvm` Book loader (ast/src/parser.rs),
+// label sets (host/src/calc_labels.rs), Def encoding (host/src/encode.rs)
+// into the flat device instruction table, and readback of a device heap image
+// (host/src/readback.rs) into the text format (ast/src/ast.rs Display).
+#pragma once
+#include <stdint.h>
+
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "num.h"
+
+namespace hvm {
+
+// ---- ports (runtime/src/port.rs:20-224), identical 64-bit layout ----------
+// tag bits 0-2, address bits 3-47 (a byte offset into the device heap, so the
+// other half of a node is addr ^ 8), label bits 48-63.  A Ref port's address
+// is (def id + 1) << 3; an expansion agent's address has bit 47 set and names
+// the heap word holding its output port.
+enum PortTag : uint8_t { T_RED = 0, T_VAR = 1, T_REF = 2, T_NUM = 3, T_OP = 5, T_SWITCH = 6, T_CTR = 7 };
+constexpr uint64_t PORT_ERA = 2;
+constexpr uint64_t PORT_FREE = 0x8000000000000000ull;
+constexpr uint64_t PORT_LOCK = 0xFFFFFFFFFFFFFFF0ull;
+constexpr uint64_t PORT_GONE = 0xFFFFFFFFFFFFFFFFull;
+constexpr uint64_t ADDR_MASK = 0x0000FFFFFFFFFFF8ull;
+constexpr uint64_t EXPAND_BIT = 1ull << 47;
+
+inline uint64_t port_new(uint8_t tag, uint16_t lab, uint64_t addr) { return (uint64_t(lab) << 48) | addr | tag; }
+inline uint64_t ref_port(uint32_t def_id, uint16_t min_safe) { return port_new(T_REF, min_safe, uint64_t(def_id + 1) << 3); }
+
+// ---- device instruction table -------------------------------------------
+// One Def = a run of DevInstr (the reference's Instruction list,
+// runtime/src/instruction.rs:34-72) over a small register file; TrgIds are
+// renamed to registers by linear scan (each TrgId is written once and read
+// once), register 0 being the Def's argument port.
+enum InstrKind : uint8_t { I_CONST, I_LINK, I_LINKCONST, I_CTR, I_OP, I_OPNUM, I_SWITCH, I_WIRES };
+
+struct DevInstr {  // 32 bytes
+  uint8_t k;
+  uint8_t op;    // NumTag for Op / OpNum
+  uint16_t lab;  // Ctr label
+  uint32_t a, b, c, d;
+  uint32_t pad;
+  uint64_t port;  // Const / LinkConst port, OpNum right operand (low 32 bits)
+};
+
+struct DevDef {  // 32 bytes
+  uint32_t ins_off, ins_len;
+  uint32_t nregs;
+  uint32_t lab_off, lab_len;  // label bitset words in the shared table
+  uint16_t min_safe;
+  uint16_t flags;
+  uint32_t nodes;  // upper bound on nodes one call allocates
+  uint32_t redexes;
+};
+static_assert(sizeof(DevInstr) == 32, "DevInstr layout");
+static_assert(sizeof(DevDef) == 32, "DevDef layout");
+
+constexpr uint32_t MAX_REGS = 48;  // device register file per call
+
+struct LabSet {  // runtime/src/def.rs:7-62
+  uint16_t min_safe = 0;
+  std::vector<uint64_t> bits;
+  void add(uint16_t lab);
+  bool has(uint16_t lab) const;
+  void unite(const LabSet& o);
+};
+
+// ---- AST (ast/src/ast.rs) -------------------------------------------------
+enum TreeKind : uint8_t { K_ERA, K_NUM, K_REF, K_CTR, K_OP, K_SWITCH, K_VAR };
+struct Tree {
+  TreeKind kind = K_ERA;
+  uint16_t lab = 0;
+  uint32_t num = 0;
+  std::string name;
+  Tree* p1 = nullptr;
+  Tree* p2 = nullptr;
+};
+struct Arena {
+  std::deque<Tree> nodes;
+  Tree* make(TreeKind k);
+};
+struct AstNet {
+  Tree* root = nullptr;
+  std::vector<std::pair<Tree*, Tree*>> redexes;
+};
+struct AstBook {
+  std::shared_ptr<Arena> arena = std::make_shared<Arena>();
+  std::map<std::string, AstNet> nets;
+};
+
+struct Error : std::exception {
+  int code;
+  std::string msg;
+  Error(int c, std::string m) : code(c), msg(std::move(m)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+
+AstBook parse_book(const std::string& text);
+AstNet parse_net(const std::string& text, Arena& arena);
+Tree* parse_tree(const std::string& text, Arena& arena);
+std::string print_tree(const Tree* t);
+std::string print_net(const AstNet& n);
+std::string num_to_string(uint32_t n);
+void apply_tree(AstNet& net, Tree* arg, Arena& arena);
+
+// ---- a loaded Book: names, label sets and the device tables ---------------
+struct Book {
+  std::vector<std::string> names;  // def id -> name
+  std::map<std::string, uint32_t> ids;
+  std::vector<LabSet> labs;
+  std::vector<DevDef> defs;  // Book defs first, then expression programs
+  std::vector<DevInstr> instrs;
+  std::vector<uint64_t> labbits;
+  std::vector<std::shared_ptr<Arena>> keep;
+
+  // Loads a Book (Host::insert_book, host/src/host.rs:34-73).
+  void load(const AstBook& b);
+  // Encodes an expression net as a program run against the root
+  // (Host::encode_net, host/src/encode.rs:116-120).  Returns its def index.
+  uint32_t add_expr(const AstNet& net);
+  uint32_t def_count() const { return uint32_t(names.size()); }
+};
+
+// Reads the net rooted at heap word `root` out of a heap image
+// (Host::readback, host/src/readback.rs:23-87).  Redirect chains (Red ports
+// left by concurrent linking) are followed to the live endpoint.
+std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root);
+
+// Runs f on a thread with a large stack (deep trees recurse; the reference
+// grows its stack with `stacker`, util/src/maybe_grow.rs).
+void with_big_stack(const std::function<void()>& f);
+
+}  // namespace hvm

@@ -1,0 +1,107 @@
+/*
+ * hvm64.h -- C ABI of the B200 interaction-net reducer.
+ *
+ * Drop-in boundary for HVM-64 net normalisation.  The reference's boundary is
+ * a Rust API (no C ABI); each entry point below names the reference call it
+ * replaces.  Paths are relative to the HigherOrderCO/hvm-64 checkout.
+ *
+ * Conventions
+ *  - Every call returns an int status: HVM64_OK (0) or an HVM64_ERR_* code,
+ *    where the reference would panic or abort.  hvm64_last_error() gives the
+ *    message of the last failure on the calling thread.
+ *  - Handles are owned by the caller and released with the *_free calls.
+ *    One handle is used by one host thread at a time (the reference's
+ *    `&mut Net`).
+ *  - A net's heap, redex queue and Book tables live in device memory behind
+ *    the handle; buffers in these signatures are host memory.
+ *  - No torch or CUDA types appear here; the library picks the current CUDA
+ *    device at hvm64_net_create / hvm64_batch_create.
+ */
+#ifndef HVM64_H
+#define HVM64_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HVM64_OK 0
+#define HVM64_ERR_OOM 1       /* heap exhausted: runtime/src/allocator.rs:104 expect("OOM") */
+#define HVM64_ERR_BAD_PAIR 2  /* no rule for the pair: runtime/src/interact.rs:39-42 */
+#define HVM64_ERR_DIV0 3      /* integer / or % by zero: num/src/num.rs:183-186,209-212 */
+#define HVM64_ERR_TIMEOUT 4   /* a bounded device wait or the run deadline ran out */
+#define HVM64_ERR_BAD_INPUT 5 /* parse error, unknown reference, bad argument */
+#define HVM64_ERR_CUDA 6      /* CUDA runtime error (no device, launch failure) */
+#define HVM64_ERR_QUEUE 7     /* the device redex queue overflowed */
+#define HVM64_ERR_BAD_ADDR 8  /* a heap address outside the arena (internal fault, caught) */
+
+/* Per-rule interaction counters: runtime/src/runtime.rs:72-79 (Rewrites). */
+typedef struct hvm64_rewrites {
+  uint64_t anni, comm, eras, dref, oper;
+} hvm64_rewrites;
+
+/* Device launch knobs (0 = default).  The autotuner sweeps these. */
+typedef struct hvm64_tuning {
+  uint32_t blocks_per_sm;    /* resident reducer blocks per SM (8 warps each) */
+  uint32_t chunk_nodes;      /* nodes a lane takes from the global bump at once */
+  uint32_t donate_min;       /* warp-stack depth above which a warp shares work */
+  uint32_t queue_slots_log2; /* global redex-queue capacity, in 32-redex slots */
+  uint64_t timeout_ms;       /* run deadline; a longer run fails with TIMEOUT */
+} hvm64_tuning;
+
+typedef struct hvm64_book hvm64_book;
+typedef struct hvm64_net hvm64_net;
+typedef struct hvm64_batch hvm64_batch;
+
+const char* hvm64_last_error(void);
+const char* hvm64_version(void);
+
+/* Book::from_str + Host::new (ast/src/parser.rs:464-469, host/src/host.rs:25-73):
+ * parse `.hvm` text, compute label sets, encode every Def. */
+int hvm64_book_load(const char* text, size_t len, hvm64_book** out);
+/* Number of Defs, and the name of Def `i` (host/src/host.rs:19-21). */
+uint32_t hvm64_book_def_count(const hvm64_book* book);
+const char* hvm64_book_def_name(const hvm64_book* book, uint32_t i);
+void hvm64_book_free(hvm64_book* book);
+
+/* Heap::new(bytes) + Net::new (runtime/src/allocator.rs:22, runtime/src/net.rs:19).
+ * heap_bytes = 0 picks a default sized from free device memory. */
+int hvm64_net_create(const hvm64_book* book, uint64_t heap_bytes, hvm64_net** out);
+/* Net::boot(&host.defs[name]) (runtime/src/net.rs:30-32): the root is bound to
+ * a call of the named Def (counts one DREF). */
+int hvm64_net_boot(hvm64_net* net, const char* def_name);
+/* Host::encode_net(net, root, &ast_net) (host/src/encode.rs:116-120): the root
+ * is bound to an expression net written in the text format. */
+int hvm64_net_encode(hvm64_net* net, const char* net_text, size_t len);
+/* Net::normal / Net::parallel_normal (runtime/src/net.rs:55-60,
+ * runtime/src/parallel.rs:35-160): expand and reduce to normal form on the
+ * device.  `out` receives net.rwts; `device_ms` (nullable) the device time. */
+int hvm64_net_normal(hvm64_net* net, const hvm64_tuning* tuning, hvm64_rewrites* out, double* device_ms);
+/* Host::readback + Display (host/src/readback.rs:23-33, ast/src/ast.rs:234-263).
+ * Writes at most cap bytes (NUL-terminated when it fits) and sets *len to the
+ * full text length; call with cap = 0 to size the buffer. */
+int hvm64_net_readback(hvm64_net* net, char* buf, size_t cap, size_t* len);
+void hvm64_net_free(hvm64_net* net);
+
+/* Batched normalisation: `n` independent nets, each booted from Def
+ * entries[i] (Net::boot) or, when entries[i] starts with '=', encoded from the
+ * expression text after it (Host::encode_net), all reduced together in one
+ * persistent launch.  No reference counterpart: the reference normalises one
+ * net per call (src/main.rs:176-193). */
+int hvm64_batch_create(const hvm64_book* book, uint32_t n, const char* const* entries, uint64_t heap_bytes,
+                       hvm64_batch** out);
+#define HVM64_BATCH_PERSISTENT 0 /* all nets in one persistent launch */
+#define HVM64_BATCH_PLAIN 1      /* one net per launch, one after the other */
+/* Reduce every net.  per_net (n entries, nullable) receives each net's
+ * counters, status (n entries, nullable) each net's status code. */
+int hvm64_batch_normal(hvm64_batch* batch, int mode, const hvm64_tuning* tuning, hvm64_rewrites* per_net,
+                       int* status, double* device_ms);
+int hvm64_batch_readback(hvm64_batch* batch, uint32_t i, char* buf, size_t cap, size_t* len);
+void hvm64_batch_free(hvm64_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HVM64_H */
