@@ -19,6 +19,12 @@
 #pragma once
 #include <stdint.h>
 
+#ifndef __CUDACC__
+#include <atomic>
+#include <chrono>
+#include <thread>
+#endif
+
 #include "host.hpp"
 #include "hvm64.h"
 #include "num.h"
@@ -52,6 +58,7 @@ struct Ctrl {
   ull spin_limit;
   ull deadline;    // %globaltimer ns
   ull donate_min;
+  ull lane_budget;
   ull q_mask;
   int error;
   int error_net;
@@ -68,10 +75,13 @@ struct Ctrl {
   ull stat_donated, stat_spilled, stat_overflow, stat_taken;
 };
 
-struct NetState {  // 64 bytes
+constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
+enum : int { EX_COMM22 = 5, EX_DNODES, EX_DLINKS };
+
+struct NetState {  // 96 bytes
   ull root;            // byte offset of the root wire
   long long pending;   // warps holding this net's work + queued chunks
-  ull rw[5];
+  ull rw[NCOUNT];
   int prog;            // DevDef index of the boot program
   int status;
 };
@@ -96,7 +106,15 @@ struct Params {
   unsigned ndefs;
 };
 
-// ---- strong memory operations --------------------------------------------
+// ---- platform layer ------------------------------------------------------------
+// The runtime below is written against these few operations.  Under nvcc
+// they are strong GPU-scope PTX accesses and CUDA atomics; under a host
+// compiler (the CPU emulation harness the tests build from this same file)
+// they are std::atomic_ref operations, so the protocol logic can be exercised
+// with many host threads.
+#ifdef __CUDACC__
+#define HVM_DEV __device__
+#define HVM_INL __device__ __forceinline__
 __device__ __forceinline__ ull ld_gpu(const ull* p) {
   ull v;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -110,57 +128,127 @@ __device__ __forceinline__ int ld_gpu32(const int* p) {
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ long long ld_gpu64s(const long long* p) {
-  return (long long)ld_gpu(reinterpret_cast<const ull*>(p));
-}
 __device__ __forceinline__ ull globaltimer() {
   ull t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+__device__ __forceinline__ ull atom_exch(ull* p, ull v) { return atomicExch(p, v); }
+__device__ __forceinline__ ull atom_cas(ull* p, ull e, ull v) { return atomicCAS(p, e, v); }
+__device__ __forceinline__ ull atom_add(ull* p, ull v) { return atomicAdd(p, v); }
+__device__ __forceinline__ int atom_cas32(int* p, int e, int v) { return atomicCAS(p, e, v); }
+__device__ __forceinline__ void mem_fence() { __threadfence(); }
+__device__ __forceinline__ void pause_brief() { __nanosleep(64); }
+// LOCK-fill nodes [s, s+n) with 16-byte stores.
+__device__ __forceinline__ void lock_fill(ull* H, ull s, ull n) {
+  ulonglong2* c = reinterpret_cast<ulonglong2*>(H) + s;
+  for (ull k = 0; k < n; k++) c[k] = make_ulonglong2(P_LOCK, P_LOCK);
+}
+#else
+#define HVM_DEV
+#define HVM_INL inline
+#ifdef HVM_EMU_STRESS
+// Test builds only: yield at random inside memory operations to widen race
+// windows.
+inline void emu_jitter() {
+  thread_local unsigned x = 0x9E3779B9u ^ unsigned(std::hash<std::thread::id>{}(std::this_thread::get_id()));
+  x ^= x << 13; x ^= x >> 17; x ^= x << 5;
+  if ((x & 31) == 0) std::this_thread::yield();
+}
+#else
+inline void emu_jitter() {}
+#endif
+inline ull ld_gpu(const ull* p) {
+  emu_jitter();
+  return std::atomic_ref<ull>(*const_cast<ull*>(p)).load(std::memory_order_acquire);
+}
+inline void st_gpu(ull* p, ull v) {
+  emu_jitter();
+  std::atomic_ref<ull>(*p).store(v, std::memory_order_release);
+}
+inline int ld_gpu32(const int* p) {
+  return std::atomic_ref<int>(*const_cast<int*>(p)).load(std::memory_order_acquire);
+}
+inline ull globaltimer() {
+  return ull(std::chrono::duration_cast<std::chrono::nanoseconds>(
+                 std::chrono::steady_clock::now().time_since_epoch()).count());
+}
+inline ull atom_exch(ull* p, ull v) {
+  emu_jitter();
+  return std::atomic_ref<ull>(*p).exchange(v);
+}
+inline ull atom_cas(ull* p, ull e, ull v) {
+  emu_jitter();
+  std::atomic_ref<ull>(*p).compare_exchange_strong(e, v);
+  return e;
+}
+inline ull atom_add(ull* p, ull v) { return std::atomic_ref<ull>(*p).fetch_add(v); }
+inline int atom_cas32(int* p, int e, int v) {
+  std::atomic_ref<int>(*p).compare_exchange_strong(e, v);
+  return e;
+}
+inline void mem_fence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+inline void pause_brief() { std::this_thread::yield(); }
+inline void lock_fill(ull* H, ull s, ull n) {
+  for (ull k = 0; k < 2 * n; k++) st_gpu(H + 2 * s + k, P_LOCK);
+}
+#endif
+HVM_INL long long ld_gpu64s(const long long* p) {
+  return (long long)ld_gpu(reinterpret_cast<const ull*>(p));
+}
 
 // ---- ports (runtime/src/port.rs) ---------------------------------------------
-__device__ __forceinline__ unsigned ptag(ull p) { return unsigned(p & 7); }
-__device__ __forceinline__ unsigned plab(ull p) { return unsigned(p >> 48); }
-__device__ __forceinline__ ull paddr(ull p) { return p & A_MASK; }
-__device__ __forceinline__ ull mkport(unsigned tag, unsigned lab, ull addr) { return (ull(lab) << 48) | addr | tag; }
-__device__ __forceinline__ ull pvar(ull a) { return a | T_VAR; }
-__device__ __forceinline__ ull pred(ull a) { return a | T_RED; }
-__device__ __forceinline__ bool principal(ull p) { return ptag(p) >= T_REF; }
-__device__ __forceinline__ bool skippable(ull p) {  // port.rs:205-207
+HVM_INL unsigned ptag(ull p) { return unsigned(p & 7); }
+HVM_INL unsigned plab(ull p) { return unsigned(p >> 48); }
+HVM_INL ull paddr(ull p) { return p & A_MASK; }
+HVM_INL ull mkport(unsigned tag, unsigned lab, ull addr) { return (ull(lab) << 48) | addr | tag; }
+HVM_INL ull pvar(ull a) { return a | T_VAR; }
+HVM_INL ull pred(ull a) { return a | T_RED; }
+HVM_INL bool principal(ull p) { return ptag(p) >= T_REF; }
+HVM_INL bool skippable(ull p) {  // port.rs:205-207
   return ptag(p) == T_NUM || (ptag(p) == T_REF && plab(p) != 0xFFFF);
 }
-__device__ __forceinline__ bool is_expand(ull p) { return ptag(p) == T_REF && (p & X_BIT) != 0; }
+HVM_INL bool is_expand(ull p) { return ptag(p) == T_REF && (p & X_BIT) != 0; }
 // Trg (runtime/src/linker.rs:228-281): a wire is its address with the Red tag.
-__device__ __forceinline__ bool trg_is_wire(ull t) { return ptag(t) == T_RED; }
+HVM_INL bool trg_is_wire(ull t) { return ptag(t) == T_RED; }
+
+constexpr int FLCAP = 32;  // per-lane stack of ready (LOCK-filled) free nodes
+constexpr int FWCAP = 8;   // words freed by the current interaction, awaiting their other half
 
 struct Lane {
   const Params& P;
   ull* H;
   ull hb;
-  ull head;   // free-list head (byte address; 0 = empty)
-  ull bnext;  // bump chunk [bnext, bend) in node indices
+  ull ovf;    // overflow free list (left word links; right word LOCK)
+  ull bnext;  // pre-LOCKed bump chunk [bnext, bend) in node indices
   ull bend;
-  ull rw[5];
+  ull allocs;  // nodes allocated by this lane
+  ull rw[NCOUNT];
   unsigned net;
   int pn;
+  int fln;
+  int fwn;
+  bool dirty;  // recycled nodes whose LOCK fill has not been fenced yet
   ull pb[2 * LBCAP];
+  ull fl[FLCAP];
+  ull fw[FWCAP];
 
-  __device__ explicit Lane(const Params& p) : P(p), H(p.heap), hb(p.ctrl->heap_bytes), head(0), bnext(0), bend(0),
-                                              net(0), pn(0) {
-    for (int k = 0; k < 5; k++) rw[k] = 0;
+  HVM_DEV explicit Lane(const Params& p)
+      : P(p), H(p.heap), hb(p.ctrl->heap_bytes), ovf(0), bnext(0), bend(0), allocs(0), net(0), pn(0), fln(0),
+        fwn(0), dirty(false) {
+    for (int k = 0; k < NCOUNT; k++) rw[k] = 0;
   }
 
-  __device__ void fail(int code, ull info) {
-    if (atomicCAS(&P.ctrl->error, 0, code) == 0) {
+  HVM_DEV void fail(int code, ull info) {
+    if (atom_cas32(&P.ctrl->error, 0, code) == 0) {
       P.ctrl->error_info = info;
       P.ctrl->error_net = int(net);
     }
   }
-  __device__ bool failed() const { return ld_gpu32(&P.ctrl->error) != 0; }
+  HVM_DEV bool failed() const { return ld_gpu32(&P.ctrl->error) != 0; }
 
   // One poll of a bounded wait; false = abandon the wait.
-  __device__ bool spin(unsigned& it) {
+  HVM_DEV bool spin(unsigned& it) {
     ++it;
     if ((it & 63) == 0) {
       if (failed()) return false;
@@ -168,25 +256,25 @@ struct Lane {
         fail(HVM64_ERR_TIMEOUT, 0);
         return false;
       }
-      __nanosleep(64);
+      pause_brief();
     }
     return true;
   }
 
-  __device__ ull* at(ull a) {
+  HVM_DEV ull* at(ull a) {
     if (a >= hb) {
       fail(HVM64_ERR_BAD_ADDR, a);
       a = 0;
     }
     return H + (a >> 3);
   }
-  __device__ ull load(ull a) { return ld_gpu(at(a)); }
-  __device__ void store(ull a, ull v) { st_gpu(at(a), v); }
-  __device__ ull swap(ull a, ull v) { return atomicExch(at(a), v); }
-  __device__ ull cas(ull a, ull e, ull v) { return atomicCAS(at(a), e, v); }
+  HVM_DEV ull load(ull a) { return ld_gpu(at(a)); }
+  HVM_DEV void store(ull a, ull v) { st_gpu(at(a), v); }
+  HVM_DEV ull swap(ull a, ull v) { return atom_exch(at(a), v); }
+  HVM_DEV ull cas(ull a, ull e, ull v) { return atom_cas(at(a), e, v); }
 
   // wire.rs:342-350
-  __device__ ull lock_target(ull w) {
+  HVM_DEV ull relock(ull w) {
     unsigned it = 0;
     for (;;) {
       ull got = swap(w, P_LOCK);
@@ -194,58 +282,112 @@ struct Lane {
       if (!spin(it)) return P_ERA;
     }
   }
+  HVM_DEV ull lock_target(ull w) {
+    ull got = swap(w, P_LOCK);
+    return got != P_LOCK ? got : relock(w);
+  }
 
-  // ---- allocator (runtime/src/allocator.rs:73-110) --------------------------
-  __device__ void half_free(ull a) {
+  // ---- allocator -------------------------------------------------------------
+  // The reference's allocator (runtime/src/allocator.rs:73-110) writes LOCK
+  // into both words of every node it hands out and links a node into a
+  // free list once both halves are FREE.  Here a node is LOCK-filled when it
+  // becomes free (or when its bump chunk is taken) and that fill is fenced
+  // before the node is handed out again, so alloc() itself touches no memory.
+  // A node whose two halves are both freed by the same interaction is
+  // reclaimed without reading the other half.  Otherwise the reference's
+  // store-FREE / read-other-half / CAS sequence decides which lane reclaims.
+  HVM_DEV void recycle(ull node) {
+    if (fln < FLCAP) {
+      fl[fln++] = node;
+      dirty = true;
+    } else {
+      store(node, ovf);  // right word already LOCK
+      ovf = node;
+    }
+  }
+  HVM_DEV void half_free(ull a) {
+    for (int k = 0; k < fwn; k++) {
+      if (fw[k] == (a ^ 8)) {  // both halves freed by this interaction: no one else can claim the node
+        fw[k] = fw[--fwn];
+        ull l = a & ~8ull;
+        store(l, P_LOCK);
+        store(l | 8, P_LOCK);
+        recycle(l);
+        return;
+      }
+    }
     store(a, P_FREE);
     if (load(a ^ 8) == P_FREE) {
       ull l = a & ~8ull;
-      if (cas(l, P_FREE, head) == P_FREE) head = l;
-    }
-  }
-  __device__ ull alloc() {
-    ull a;
-    if (head != 0) {
-      a = head;
-      head = load(a);
-    } else {
-      if (bnext == bend) {
-        ull n = P.ctrl->chunk_nodes;
-        ull s = atomicAdd(&P.ctrl->bump, n);
-        if (s + n > P.ctrl->heap_nodes) {
-          fail(HVM64_ERR_OOM, s);
-          return 0;
+      if (cas(l, P_FREE, P_LOCK) == P_FREE) {
+        // The node may have been reclaimed and reused since the load (ABA):
+        // keep it only if its right word is still free, else hand the left
+        // word back.
+        if (load(l | 8) == P_FREE) {
+          store(l | 8, P_LOCK);
+          recycle(l);
+        } else {
+          store(l, P_FREE);
         }
-        bnext = s;
-        bend = s + n;
       }
-      a = (bnext++) << 4;
+      return;
     }
-    store(a, P_LOCK);
-    store(a ^ 8, P_LOCK);
-    __threadfence();  // LOCK is visible before the node's address escapes
-    return a;
+    if (fwn == FWCAP) fwn = 0;
+    fw[fwn++] = a;
+  }
+  // End of an interaction: later frees of the other halves take the
+  // ordinary path.
+  HVM_DEV void settle() { fwn = 0; }
+  HVM_DEV ull alloc() {
+    allocs++;
+    if (fln > 0) {
+      if (dirty) {
+        mem_fence();
+        dirty = false;
+      }
+      return fl[--fln];
+    }
+    if (ovf != 0) {
+      ull a = ovf;
+      ovf = load(a);
+      store(a, P_LOCK);
+      mem_fence();
+      return a;
+    }
+    if (bnext == bend) {
+      ull n = P.ctrl->chunk_nodes;
+      ull s = atom_add(&P.ctrl->bump, n);
+      if (s + n > P.ctrl->heap_nodes) {
+        fail(HVM64_ERR_OOM, s);
+        return 0;
+      }
+      lock_fill(H, s, n);
+      mem_fence();  // LOCK is visible before any of these nodes escapes
+      bnext = s;
+      bend = s + n;
+    }
+    return (bnext++) << 4;
   }
 
   // ---- redex pushes ----------------------------------------------------------
-  __device__ void overflow();
-  __device__ void push(ull a, ull b) {
+  HVM_DEV void overflow();
+  HVM_DEV void push(ull a, ull b) {
     if (pn == LBCAP) overflow();
     pb[2 * pn] = a;
     pb[2 * pn + 1] = b;
     pn++;
   }
   // linker.rs:70-85
-  __device__ void redux(ull a, ull b) {
+  HVM_DEV void redux(ull a, ull b) {
     if (skippable(a) && skippable(b)) rw[RW_ERAS]++;
     else push(a, b);
   }
 
   // ---- linker (runtime/src/linker.rs:25-203) --------------------------------
-  __device__ void half_link_port_port(ull a, ull b) {
+  HVM_DEV void half_link_port_port(ull a, ull b) {
     if (ptag(a) == T_VAR) store(paddr(a), b);
   }
-  __device__ void link_port_port(ull a, ull b) {
+  HVM_DEV void link_port_port(ull a, ull b) {
     if (principal(a) && principal(b)) {
       redux(a, b);
     } else {
@@ -253,7 +395,9 @@ struct Lane {
       half_link_port_port(b, a);
     }
   }
-  __device__ void link_wire_wire(ull aw, ull bw) {
+  HVM_DEV void link_wire_wire(ull aw, ull bw) {
+    // Lock order as in the reference: a lane waiting on `aw` must not hold
+    // `bw`, or a lane resolving a redirect through `bw` could wait on it.
     ull ap = lock_target(aw);
     ull bp = lock_target(bw);
     if (principal(ap) && principal(bp)) {
@@ -265,7 +409,7 @@ struct Lane {
       half_link_wire_port(bp, bw, ap);
     }
   }
-  __device__ void link_wire_port(ull aw, ull bp) {
+  HVM_DEV void link_wire_port(ull aw, ull bp) {
     ull ap = lock_target(aw);
     if (principal(ap) && principal(bp)) {
       half_free(aw);
@@ -275,7 +419,7 @@ struct Lane {
       half_link_port_port(bp, ap);
     }
   }
-  __device__ void half_link_wire_port(ull ap, ull aw, ull bp) {
+  HVM_DEV void half_link_wire_port(ull ap, ull aw, ull bp) {
     if (ptag(ap) == T_VAR) {
       if (cas(paddr(ap), pvar(aw), bp) == pvar(aw)) {
         half_free(aw);
@@ -291,7 +435,7 @@ struct Lane {
       half_free(aw);
     }
   }
-  __device__ void resolve_redirect_pri(ull ap, ull aw, ull bp) {
+  HVM_DEV void resolve_redirect_pri(ull ap, ull aw, ull bp) {
     unsigned it = 0;
     for (;;) {
       ull tw = paddr(ap);
@@ -341,31 +485,32 @@ struct Lane {
       return;
     }
   }
-  __device__ void link_trg_port(ull a, ull b) {
+  HVM_DEV void link_trg_port(ull a, ull b) {
     if (trg_is_wire(a)) link_wire_port(a, b);
     else link_port_port(a, b);
   }
-  __device__ void link_trg(ull a, ull b) {
+  HVM_DEV void link_trg(ull a, ull b) {
     bool aw = trg_is_wire(a), bw = trg_is_wire(b);
     if (aw && bw) link_wire_wire(a, b);
     else if (aw) link_wire_port(a, b);
     else if (bw) link_wire_port(b, a);
     else link_port_port(a, b);
   }
-  __device__ ull trg_target(ull t) { return trg_is_wire(t) ? load(t) : t; }
-  __device__ void free_trg(ull t) {
+  HVM_DEV ull trg_target(ull t) { return trg_is_wire(t) ? load(t) : t; }
+  HVM_DEV void free_trg(ull t) {
     if (trg_is_wire(t)) half_free(t);
   }
 
   // ---- rules (runtime/src/interact.rs) ----------------------------------------
-  __device__ void anni2(ull a, ull b) {  // interact.rs:72-79
+  HVM_DEV void anni2(ull a, ull b) {  // interact.rs:72-79
     rw[RW_ANNI]++;
     ull a1 = paddr(a), b1 = paddr(b);
     link_wire_wire(a1, b1);
     link_wire_wire(a1 ^ 8, b1 ^ 8);
   }
-  __device__ void comm22(ull a, ull b) {  // interact.rs:118-141
+  HVM_DEV void comm22(ull a, ull b) {  // interact.rs:118-141
     rw[RW_COMM]++;
+    rw[EX_COMM22]++;
     ull a1 = paddr(a), b1 = paddr(b);
     ull A1 = alloc(), A2 = alloc(), B1 = alloc(), B2 = alloc();
     unsigned ta = ptag(a), la = plab(a), tb = ptag(b), lb = plab(b);
@@ -378,13 +523,13 @@ struct Lane {
     link_wire_port(b1, mkport(ta, la, A1));
     link_wire_port(b1 ^ 8, mkport(ta, la, A2));
   }
-  __device__ void comm02(ull a, ull b) {  // interact.rs:162-168
+  HVM_DEV void comm02(ull a, ull b) {  // interact.rs:162-168
     rw[RW_COMM]++;
     ull b1 = paddr(b);
     link_wire_port(b1, a);
     link_wire_port(b1 ^ 8, a);
   }
-  __device__ void switch_num(ull a, ull b) {  // interact.rs:201-223
+  HVM_DEV void switch_num(ull a, ull b) {  // interact.rs:201-223
     rw[RW_OPER]++;
     ull a1 = paddr(a);
     uint32_t num = uint32_t(b);
@@ -403,13 +548,13 @@ struct Lane {
       link_wire_port(a1, mkport(T_CTR, 0, x));
     }
   }
-  __device__ uint32_t binary(uint32_t a, uint32_t op, uint32_t b) {
+  HVM_DEV uint32_t binary(uint32_t a, uint32_t op, uint32_t b) {
     int e = 0;
     uint32_t r = num_binary(a, op, b, &e);
     if (e) fail(HVM64_ERR_DIV0, net);
     return r;
   }
-  __device__ void op_num(ull a, ull b) {  // interact.rs:251-270
+  HVM_DEV void op_num(ull a, ull b) {  // interact.rs:251-270
     uint32_t op = plab(a);
     ull a1 = paddr(a);
     ull t1 = load(a1);
@@ -427,7 +572,7 @@ struct Lane {
   }
 
   // def.rs:30-37 (LabSet::has); the expansion agent's set is LabSet::ALL.
-  __device__ bool def_has(ull ref, unsigned lab) {
+  HVM_DEV bool def_has(ull ref, unsigned lab) {
     if (ref & X_BIT) return lab < 0xFFFF;
     unsigned id = unsigned((paddr(ref) >> 3) - 1);
     if (id >= P.ndefs) {
@@ -441,15 +586,17 @@ struct Lane {
     return (P.labbits[d.lab_off + w] >> (lab & 63)) & 1;
   }
   // def.rs:177-189
-  __device__ void call(ull port, ull trg) {
+  HVM_DEV void call(ull port, ull trg) {
     if (ptag(trg) == T_CTR && !def_has(port, plab(trg))) return comm02(port, trg);
     rw[RW_DREF]++;
-    if (port & X_BIT) expand_call(port, trg);
-    else run_def(unsigned((paddr(port) >> 3) - 1), trg);
+    if (port & X_BIT) return expand_call(port, trg);
+    ull before = allocs;
+    run_def(unsigned((paddr(port) >> 3) - 1), trg);
+    rw[EX_DNODES] += allocs - before;
   }
 
   // ---- interact.rs:6-44 --------------------------------------------------------
-  __device__ void interact(ull a, ull b) {
+  HVM_DEV void interact(ull a, ull b) {
     unsigned at = ptag(a), bt = ptag(b);
     if (at <= T_VAR || bt <= T_VAR) return fail(HVM64_ERR_BAD_PAIR, a);
     bool an = at == T_REF || at == T_NUM, bn = bt == T_REF || bt == T_NUM;
@@ -480,7 +627,7 @@ struct Lane {
   }
 
   // ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) ----
-  __device__ void do_ctr(unsigned lab, ull trg, ull& o1, ull& o2) {
+  HVM_DEV void do_ctr(unsigned lab, ull trg, ull& o1, ull& o2) {
     ull port = trg_target(trg);
     if (ptag(port) == T_CTR && plab(port) == lab) {
       free_trg(trg);
@@ -494,7 +641,7 @@ struct Lane {
     o1 = pvar(n);
     o2 = pvar(n ^ 8);
   }
-  __device__ void do_op(unsigned op, ull trg, ull& o1, ull& o2) {
+  HVM_DEV void do_op(unsigned op, ull trg, ull& o1, ull& o2) {
     ull port = trg_target(trg);
     if (ptag(port) == T_NUM) {
       free_trg(trg);
@@ -514,7 +661,7 @@ struct Lane {
     o1 = pvar(n);
     o2 = pvar(n ^ 8);
   }
-  __device__ ull do_op_num(unsigned op, ull trg, uint32_t rhs) {
+  HVM_DEV ull do_op_num(unsigned op, ull trg, uint32_t rhs) {
     ull port = trg_target(trg);
     if (ptag(port) == T_NUM) {
       rw[RW_OPER]++;
@@ -530,13 +677,13 @@ struct Lane {
     store(n, ull(rhs));
     return pvar(n ^ 8);
   }
-  __device__ ull create_wire_to(ull port) {  // node.rs:176-182
+  HVM_DEV ull create_wire_to(ull port) {  // node.rs:176-182
     ull a = alloc();
     half_free(a ^ 8);
     link_port_port(port, pvar(a));
     return a;
   }
-  __device__ void do_switch(ull trg, ull& o1, ull& o2) {
+  HVM_DEV void do_switch(ull trg, ull& o1, ull& o2) {
     ull port = trg_target(trg);
     if (ptag(port) == T_NUM) {
       rw[RW_OPER]++;
@@ -570,7 +717,7 @@ struct Lane {
     o2 = pvar(m ^ 8);
   }
 
-  __device__ void run_def(unsigned id, ull t0) {
+  HVM_DEV void run_def(unsigned id, ull t0) {
     if (id >= P.ndefs) return fail(HVM64_ERR_BAD_INPUT, id);
     const DevDef d = P.defs[id];
     ull R[MAX_REGS];
@@ -580,8 +727,8 @@ struct Lane {
       const DevInstr I = ins[k];
       switch (I.k) {
         case I_CONST: R[I.a] = I.port; break;
-        case I_LINK: link_trg(R[I.a], R[I.b]); break;
-        case I_LINKCONST: link_trg_port(R[I.a], I.port); break;
+        case I_LINK: rw[EX_DLINKS]++; link_trg(R[I.a], R[I.b]); break;
+        case I_LINKCONST: rw[EX_DLINKS]++; link_trg_port(R[I.a], I.port); break;
         case I_CTR: {
           ull x, y;
           do_ctr(I.lab, R[I.a], x, y);
@@ -619,13 +766,13 @@ struct Lane {
   // ---- expansion agent (runtime/src/net.rs:63-108) ----------------------------
   // An agent is a Ref port with X_BIT whose address names a heap word holding
   // its output port (the reference boxes an `ExpandDef { out }`).
-  __device__ ull new_expand(ull out) {
+  HVM_DEV ull new_expand(ull out) {
     ull w = alloc();
     half_free(w ^ 8);
     store(w, out);
     return mkport(T_REF, 0xFFFF, X_BIT | w);
   }
-  __device__ ull take_expand(ull port) {
+  HVM_DEV ull take_expand(ull port) {
     ull w = paddr(port) & ~X_BIT;
     unsigned it = 0;
     ull out;
@@ -634,7 +781,7 @@ struct Lane {
     half_free(w);
     return out;
   }
-  __device__ void expand_call(ull self, ull port) {
+  HVM_DEV void expand_call(ull self, ull port) {
     if (ptag(port) == T_REF && port != P_ERA) {
       if (port & X_BIT) {
         ull a = take_expand(self), b = take_expand(port);
@@ -653,7 +800,7 @@ struct Lane {
     link_wire_port(o1 ^ 8, new_expand(pvar(n ^ 8)));
   }
   // net.rs:65-69
-  __device__ ull expand(ull root) {
+  HVM_DEV ull expand(ull root) {
     ull a = alloc();
     half_free(a ^ 8);
     link_wire_port(root, new_expand(pvar(a)));

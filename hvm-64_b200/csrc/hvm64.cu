@@ -130,10 +130,11 @@ __device__ bool donate(const Params& P, Lane& L, ull* S, unsigned& bot, unsigned
   return true;
 }
 
-// Flush a warp's per-lane counters into its net (warp reduction, 5 atomics).
+// Flush a warp's per-lane counters into its net (warp reduction, one atomic
+// per counter).
 __device__ void flush_counters(const Params& P, Lane& L, int cur) {
   const unsigned lane = threadIdx.x & 31;
-  for (int k = 0; k < 5; k++) {
+  for (int k = 0; k < NCOUNT; k++) {
     ull v = L.rw[k];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0 && v) atomicAdd(&P.nets[cur].rw[k], v);
@@ -143,7 +144,9 @@ __device__ void flush_counters(const Params& P, Lane& L, int cur) {
 
 __global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
   __shared__ ull stk[WARPS][2 * SCAP];
+  __shared__ unsigned stops[WARPS];
   const unsigned lane = threadIdx.x & 31;
+  const unsigned budget0 = unsigned(P.ctrl->lane_budget);
   ull* S = stk[threadIdx.x >> 5];
   Ctrl* C = P.ctrl;
   Lane L(P);
@@ -226,7 +229,10 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
       if (__shfl_sync(0xffffffffu, late, 0)) break;
     }
 
-    // Take up to 32 redexes off the top, one per lane.
+    // Take up to 32 redexes off the top, one per lane.  A lane then keeps
+    // reducing: first the newest redex its own interactions made, else one
+    // more from the warp's stack, until its budget for this step is spent.
+    // Nothing is pushed to the stack during the step, so lanes only pop.
     unsigned n = min(top - bot, 32u);
     ull a = 0, b = 0;
     if (lane < n) {
@@ -234,9 +240,32 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
       a = S[2 * k];
       b = S[2 * k + 1];
     }
-    top -= n;
+    if (lane == 0) stops[threadIdx.x >> 5] = top - n;
     __syncwarp();
-    if (lane < n) L.interact(a, b);
+    if (lane < n) {
+      unsigned budget = budget0;
+      for (;;) {
+        L.interact(a, b);
+        L.settle();
+        if (--budget == 0) break;
+        if (L.pn > 0) {
+          L.pn--;
+          a = L.pb[2 * L.pn];
+          b = L.pb[2 * L.pn + 1];
+          continue;
+        }
+        unsigned old = atomicSub(&stops[threadIdx.x >> 5], 1u);
+        if (int(old - bot) <= 0) break;
+        unsigned k = (old - 1) & (SCAP - 1);
+        a = S[2 * k];
+        b = S[2 * k + 1];
+      }
+    }
+    __syncwarp();
+    {
+      unsigned st = stops[threadIdx.x >> 5];
+      top = int(st - bot) > 0 ? st : bot;
+    }
     __syncwarp();
 
     // Append every lane's new redexes.
@@ -290,10 +319,12 @@ __global__ void boot_kernel(Params P, unsigned first, unsigned count) {
   unsigned prog = unsigned(ns.prog);
   if (prog < P.ndefs && !(P.defs[prog].flags & 1)) L.rw[RW_DREF]++;
   L.run_def(prog, pvar(root));
+  L.settle();
   root = L.expand(root);
+  L.settle();
   ns.root = root;
   if (L.pn) L.overflow();
-  for (int k = 0; k < 5; k++)
+  for (int k = 0; k < NCOUNT; k++)
     if (L.rw[k]) atomicAdd(&ns.rw[k], L.rw[k]);
   __threadfence();
   if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&P.ctrl->nets_left), 1ull);
@@ -381,6 +412,7 @@ struct Runner {
   std::vector<uint64_t> image;  // heap image for readback
   bool image_valid = false;
   bool reduced = false;
+  uint64_t h2d = 0, d2h = 0;    // bytes copied by the last run + readbacks
 
   void setup(uint64_t bytes) {
     CU(cudaGetDevice(&device));
@@ -400,6 +432,7 @@ struct Runner {
     d_instrs.alloc(book.instrs.size());
     d_labbits.alloc(book.labbits.size());
     CU(cudaMemcpy(d_defs.p, book.defs.data(), book.defs.size() * sizeof(DevDef), cudaMemcpyHostToDevice));
+    h2d += book.defs.size() * sizeof(DevDef) + book.instrs.size() * sizeof(DevInstr) + book.labbits.size() * 8;
     if (!book.instrs.empty())
       CU(cudaMemcpy(d_instrs.p, book.instrs.data(), book.instrs.size() * sizeof(DevInstr), cudaMemcpyHostToDevice));
     if (!book.labbits.empty())
@@ -445,6 +478,7 @@ struct Runner {
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
+    c.lane_budget = t.lane_budget ? t.lane_budget : 8;
     c.q_mask = (1ull << qlog2) - 1;
     // The deadline is set on the device clock right before launch.
     c.deadline = ~0ull;
@@ -457,6 +491,7 @@ struct Runner {
     if (tp) t = *tp;
     unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : 16;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
+    h2d = d2h = 0;
     heap.alloc(heap_bytes / 8);
     ctrl.alloc(1);
     nets.alloc(progs.size());
@@ -467,7 +502,9 @@ struct Runner {
     host_nets.assign(progs.size(), dev::NetState{});
     for (size_t i = 0; i < progs.size(); i++) host_nets[i].prog = int(progs[i]);
     CU(cudaMemcpy(nets.p, host_nets.data(), host_nets.size() * sizeof(dev::NetState), cudaMemcpyHostToDevice));
+    h2d += host_nets.size() * sizeof(dev::NetState);
 
+    stat_donated = stat_spilled = stat_overflow = 0;
     cudaStream_t st = 0;
     cudaEvent_t e0, e1;
     CU(cudaEventCreate(&e0));
@@ -475,6 +512,9 @@ struct Runner {
     uint64_t timeout_ms = t.timeout_ms ? t.timeout_ms : 120000;
     float total_ms = 0;
     uint64_t bump = 1;
+    // One-net-per-launch runs keep every earlier net's nodes, so they take
+    // small allocator chunks unless told otherwise.
+    if (mode == HVM64_BATCH_PLAIN && t.chunk_nodes == 0) t.chunk_nodes = 32;
     auto one = [&](unsigned first, unsigned count) {
       // One-net-per-launch runs keep earlier nets' nodes: the bump carries on.
       reset_ctrl(t, st, qlog2, bump);
@@ -489,6 +529,11 @@ struct Runner {
       CU(cudaEventElapsedTime(&ms, e0, e1));
       total_ms += ms;
       CU(cudaMemcpy(&host_ctrl, ctrl.p, sizeof host_ctrl, cudaMemcpyDeviceToHost));
+      h2d += sizeof(dev::Ctrl);
+      d2h += sizeof(dev::Ctrl);
+      stat_donated += host_ctrl.stat_donated;
+      stat_spilled += host_ctrl.stat_spilled;
+      stat_overflow += host_ctrl.stat_overflow;
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
       if (host_ctrl.error) {
         for (unsigned k = first; k < first + count; k++) host_nets[k].status = host_ctrl.error;
@@ -503,6 +548,8 @@ struct Runner {
     CU(cudaEventDestroy(e1));
     std::vector<dev::NetState> got(progs.size());
     CU(cudaMemcpy(got.data(), nets.p, got.size() * sizeof(dev::NetState), cudaMemcpyDeviceToHost));
+    d2h += got.size() * sizeof(dev::NetState);
+    heap_used = bump;
     for (size_t i = 0; i < got.size(); i++) {
       int status = host_nets[i].status;
       host_nets[i] = got[i];
@@ -514,6 +561,22 @@ struct Runner {
   }
 
   void set_deadline(cudaStream_t st, uint64_t timeout_ms);
+  uint64_t stat_donated = 0, stat_spilled = 0, stat_overflow = 0, heap_used = 0;
+
+  void stats(hvm64_stats* o) const {
+    *o = hvm64_stats{};
+    for (const auto& n : host_nets) {
+      o->comm22 += n.rw[dev::EX_COMM22];
+      o->dref_nodes += n.rw[dev::EX_DNODES];
+      o->dref_links += n.rw[dev::EX_DLINKS];
+    }
+    o->heap_nodes_used = heap_used;
+    o->donated = stat_donated;
+    o->spilled = stat_spilled;
+    o->overflowed = stat_overflow;
+    o->h2d_bytes = h2d;
+    o->d2h_bytes = d2h;
+  }
 
   std::string readback(unsigned i) {
     if (!reduced) throw Error(HVM64_ERR_BAD_INPUT, "net not reduced yet");
@@ -525,6 +588,7 @@ struct Runner {
       used = std::min<uint64_t>(used, heap_bytes / 16);
       image.resize(used * 2);
       CU(cudaMemcpy(image.data(), heap.p, used * 16, cudaMemcpyDeviceToHost));
+      d2h += used * 16 + 8;
       image_valid = true;
     }
     std::string out;
@@ -708,5 +772,16 @@ int hvm64_batch_readback(hvm64_batch* b, uint32_t i, char* buf, size_t cap, size
   return copy_out(s, buf, cap, len);
 }
 void hvm64_batch_free(hvm64_batch* b) { delete b; }
+
+int hvm64_batch_stats(const hvm64_batch* b, hvm64_stats* out) {
+  if (!b || !out) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  b->r.stats(out);
+  return HVM64_OK;
+}
+int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
+  if (!n || !out) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  n->r.stats(out);
+  return HVM64_OK;
+}
 
 }  // extern "C"

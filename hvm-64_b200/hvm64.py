@@ -25,7 +25,7 @@ EXPORTS = (
     "hvm64_last_error", "hvm64_version", "hvm64_book_load", "hvm64_book_def_count", "hvm64_book_def_name",
     "hvm64_book_free", "hvm64_net_create", "hvm64_net_boot", "hvm64_net_encode", "hvm64_net_normal",
     "hvm64_net_readback", "hvm64_net_free", "hvm64_batch_create", "hvm64_batch_normal", "hvm64_batch_readback",
-    "hvm64_batch_free",
+    "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats",
 )
 
 
@@ -59,7 +59,16 @@ class Rewrites(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("chunk_nodes", ctypes.c_uint32),
                 ("donate_min", ctypes.c_uint32), ("queue_slots_log2", ctypes.c_uint32),
+                ("lane_budget", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
                 ("timeout_ms", ctypes.c_uint64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("comm22", "dref_nodes", "dref_links", "heap_nodes_used", "donated",
+                                                "spilled", "overflowed", "h2d_bytes", "d2h_bytes")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -95,6 +104,8 @@ def lib(build_if_missing=True):
                                      c.POINTER(c.c_double)]
     L.hvm64_batch_readback.argtypes = [P, c.c_uint32, c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_batch_free.argtypes = [P]
+    L.hvm64_batch_stats.argtypes = [P, c.POINTER(Stats)]
+    L.hvm64_net_stats.argtypes = [P, c.POINTER(Stats)]
     _lib = L
     return L
 
@@ -163,6 +174,11 @@ class Net:
     def readback(self):
         return _read_text(lib().hvm64_net_readback, self._h)
 
+    def stats(self):
+        st = Stats()
+        _check(lib().hvm64_net_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.hvm64_net_free(self._h)
@@ -195,6 +211,11 @@ class Batch:
 
     def readback(self, i):
         return _read_text(lib().hvm64_batch_readback, self._h, i)
+
+    def stats(self):
+        st = Stats()
+        _check(lib().hvm64_batch_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

@@ -48,6 +48,8 @@ typedef struct hvm64_tuning {
   uint32_t chunk_nodes;      /* nodes a lane takes from the global bump at once */
   uint32_t donate_min;       /* warp-stack depth above which a warp shares work */
   uint32_t queue_slots_log2; /* global redex-queue capacity, in 32-redex slots */
+  uint32_t lane_budget;      /* interactions a lane may do per warp step */
+  uint32_t reserved;         /* must be 0 */
   uint64_t timeout_ms;       /* run deadline; a longer run fails with TIMEOUT */
 } hvm64_tuning;
 
@@ -100,6 +102,19 @@ int hvm64_batch_normal(hvm64_batch* batch, int mode, const hvm64_tuning* tuning,
                        int* status, double* device_ms);
 int hvm64_batch_readback(hvm64_batch* batch, uint32_t i, char* buf, size_t cap, size_t* len);
 void hvm64_batch_free(hvm64_batch* batch);
+
+/* Counters of the last run, summed over the batch (no reference counterpart;
+ * the reference reports only Rewrites).  comm22 is the share of COMM done by
+ * the binary-binary rule (runtime/src/interact.rs:118-141); dref_nodes and
+ * dref_links count the nodes and links made by Def instantiation; the byte
+ * counts are the host<->device copies of the last normal + readbacks. */
+typedef struct hvm64_stats {
+  uint64_t comm22, dref_nodes, dref_links;
+  uint64_t heap_nodes_used, donated, spilled, overflowed;
+  uint64_t h2d_bytes, d2h_bytes;
+} hvm64_stats;
+int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
+int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
 
 #ifdef __cplusplus
 }

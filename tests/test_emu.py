@@ -1,0 +1,56 @@
+"""The device runtime (hvm-64_b200/csrc/device.cuh) compiled for the host and
+run on many threads with random jitter in its memory operations: the link /
+redirect protocol, the allocator and the instruction VM must give the
+reference's normal forms and counts under contention.  CPU-only."""
+import ctypes
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SO = os.path.join(HERE, "emu", "libhvm64_emu.so")
+SRC = [os.path.join(HERE, "emu", "emu.cpp"), os.path.join(ROOT, "hvm-64_b200", "csrc", "host.cpp")]
+DEPS = SRC + [os.path.join(ROOT, "hvm-64_b200", "csrc", f) for f in ("device.cuh", "host.hpp", "num.h")]
+PROGRAMS = json.load(open(os.path.join(HERE, "golden", "programs.json")))
+
+
+def _lib():
+    if not os.path.exists(SO) or any(os.path.getmtime(d) > os.path.getmtime(SO) for d in DEPS):
+        subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", "-DHVM_EMU_STRESS",
+                        "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "hvm-64_b200", "csrc"),
+                        *SRC, "-o", SO], check=True)
+    L = ctypes.CDLL(SO)
+    c = ctypes
+    L.hvm64emu_run.argtypes = [c.c_char_p, c.c_char_p, c.c_uint, c.c_uint, c.c_uint, c.c_uint64, c.c_uint64,
+                               c.POINTER(c.c_char_p), c.POINTER(c.c_uint64), c.c_char_p, c.c_size_t]
+    return L
+
+
+def emu_run(text, threads=16, budget=4, heap=256 << 20, chunk=32):
+    L = _lib()
+    out = ctypes.c_char_p()
+    rw = (ctypes.c_uint64 * 5)()
+    err = ctypes.create_string_buffer(256)
+    rc = L.hvm64emu_run(text.encode(), b"main", threads, budget, 16, heap, chunk, ctypes.byref(out), rw, err, 256)
+    assert rc == 0, err.value.decode()
+    return out.value.decode(), dict(zip(("anni", "comm", "eras", "dref", "oper"), list(rw)))
+
+
+@pytest.mark.parametrize("prog", [p for p in PROGRAMS if p["total"] <= 3_000_000], ids=lambda p: p["name"])
+def test_emu_snapshot(prog):
+    text, rw = emu_run(prog["source"])
+    assert text == prog["text"]
+    assert rw == {k: prog[k] for k in rw}
+
+
+def test_emu_workloads():
+    sys.path.insert(0, os.path.join(ROOT, "hvm-64_b200"))
+    import workloads as W
+    text, _ = emu_run(W.tree_sum(12, 3), threads=32)
+    assert text == str(W.expected_sum(12, 3))
+    text, _ = emu_run(W.bitonic(9, 4), threads=32)
+    assert W.leaves(text) == sorted(W.sort_keys(9, 4))
