@@ -34,11 +34,13 @@ namespace dev {
 
 typedef unsigned long long ull;
 
-constexpr int WARPS = 8;            // warps per reducer block
+constexpr int WARPS = 4;            // warps per reducer block
 constexpr int THREADS = WARPS * 32;
-constexpr int SCAP = 256;           // per-warp shared-memory redex stack (power of two)
-constexpr int LBCAP = 8;            // per-lane buffer of redexes made by one interaction
+constexpr int SCAP = 512;           // per-warp shared-memory redex stack (power of two)
+constexpr int HEADROOM = 192;       // stack slots kept free for the redexes of one step
 constexpr int CHUNK = 32;           // redexes per global-queue slot
+constexpr int POOL = 128;           // per-warp pool of free nodes ready for reuse
+constexpr unsigned SMALL_REGS = 12; // Defs with at most this many registers use shared memory
 
 constexpr ull P_ERA = 2;
 constexpr ull P_FREE = 0x8000000000000000ull;
@@ -73,6 +75,9 @@ struct Ctrl {
   ull q_tail;
   ull pad4[15];
   ull stat_donated, stat_spilled, stat_overflow, stat_taken;
+  ull stat_steps, stat_lanes, stat_busy_cycles, stat_idle_cycles;
+  ull timeout_ns;  // per launch: each warp's deadline is its start + timeout_ns
+  ull stat_g_steps[8], stat_g_cycles[8];  // steps by number of distinct rule classes among lanes
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -96,6 +101,7 @@ struct Slot {  // 544 bytes: one chunk of up to 32 redexes of one net
 
 struct Params {
   ull* heap;
+  ull heap_bytes;
   Ctrl* ctrl;
   NetState* nets;
   unsigned nnets;
@@ -137,6 +143,8 @@ __device__ __forceinline__ ull atom_exch(ull* p, ull v) { return atomicExch(p, v
 __device__ __forceinline__ ull atom_cas(ull* p, ull e, ull v) { return atomicCAS(p, e, v); }
 __device__ __forceinline__ ull atom_add(ull* p, ull v) { return atomicAdd(p, v); }
 __device__ __forceinline__ int atom_cas32(int* p, int e, int v) { return atomicCAS(p, e, v); }
+__device__ __forceinline__ unsigned atom_add_u32(unsigned* p, unsigned v) { return atomicAdd(p, v); }
+__device__ __forceinline__ int atom_add_i32(int* p, int v) { return atomicAdd(p, v); }
 __device__ __forceinline__ void mem_fence() { __threadfence(); }
 __device__ __forceinline__ void pause_brief() { __nanosleep(64); }
 // LOCK-fill nodes [s, s+n) with 16-byte stores.
@@ -187,6 +195,8 @@ inline int atom_cas32(int* p, int e, int v) {
   std::atomic_ref<int>(*p).compare_exchange_strong(e, v);
   return e;
 }
+inline unsigned atom_add_u32(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_add(v); }
+inline int atom_add_i32(int* p, int v) { return std::atomic_ref<int>(*p).fetch_add(v); }
 inline void mem_fence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void pause_brief() { std::this_thread::yield(); }
 inline void lock_fill(ull* H, ull s, ull n) {
@@ -212,32 +222,62 @@ HVM_INL bool is_expand(ull p) { return ptag(p) == T_REF && (p & X_BIT) != 0; }
 // Trg (runtime/src/linker.rs:228-281): a wire is its address with the Red tag.
 HVM_INL bool trg_is_wire(ull t) { return ptag(t) == T_RED; }
 
-constexpr int FLCAP = 32;  // per-lane stack of ready (LOCK-filled) free nodes
-constexpr int FWCAP = 8;   // words freed by the current interaction, awaiting their other half
+// Rule class of a redex, following interact()'s dispatch: the Def index for
+// a Def call (calls of one Def run the same instruction stream), else a small
+// code per rule.  Warps pick redexes of one class per step to stay convergent.
+HVM_INL unsigned redex_class(ull a, ull b) {
+  unsigned at = unsigned(a & 7), bt = unsigned(b & 7);
+  if (at == T_REF && !(a & X_BIT) && a != P_ERA) return 64 + unsigned((a & A_MASK) >> 3);
+  if (bt == T_REF && !(b & X_BIT) && b != P_ERA) return 64 + unsigned((b & A_MASK) >> 3);
+  if ((a & X_BIT) || (b & X_BIT)) return 1;
+  if (at == bt) return 2 + at;  // annihilation (or nilary pair)
+  return 16 + at * 8 + bt;      // commutation / native ops
+}
+
+// VM register files: a warp's shared-memory block laid out [register][lane],
+// or a local array for the rare Def needing more than SMALL_REGS.
+struct StridedRegs {
+  ull* base;
+  unsigned stride;
+  HVM_INL ull& operator[](unsigned i) const { return base[i * stride]; }
+};
+
+// Per-warp shared state of the reducer (one per warp; the CPU emulation
+// harness gives each host thread one too).
+struct WarpSmem {
+  ull stk[2 * SCAP];          // redex stack (ring of SCAP pairs)
+  ull regs[SMALL_REGS * 32];  // VM registers, [register][lane]
+  ull pool[POOL];             // free nodes ready for reuse
+  ull freed[POOL];            // nodes reclaimed during the current step
+  ull sel[64];                // the redexes chosen for the current step
+  ull rw[NCOUNT];             // counters of the warp's current net
+  ull st_steps, st_lanes, st_busy, st_idle;
+  unsigned ring_cnt;
+  int pool_n;
+  int freed_n;
+  unsigned pad;
+};
+
+HVM_INL void count(ull* c, ull v) { atom_add(c, v); }
 
 struct Lane {
   const Params& P;
-  ull* H;
-  ull hb;
-  ull ovf;    // overflow free list (left word links; right word LOCK)
-  ull bnext;  // pre-LOCKed bump chunk [bnext, bend) in node indices
+  WarpSmem* W;      // this lane's warp state (sinks, pools, counters, VM registers)
+  ull ovf;          // overflow free list (left word links; right word LOCK)
+  ull bnext;        // pre-LOCKed bump chunk [bnext, bend) in node indices
   ull bend;
-  ull allocs;  // nodes allocated by this lane
-  ull rw[NCOUNT];
+  unsigned allocs;  // nodes allocated by this lane (for the DREF statistics)
   unsigned net;
-  int pn;
-  int fln;
-  int fwn;
-  bool dirty;  // recycled nodes whose LOCK fill has not been fenced yet
-  ull pb[2 * LBCAP];
-  ull fl[FLCAP];
-  ull fw[FWCAP];
+  unsigned lane;
+  unsigned ring_base;  // this step's pushes go to stack slots ring_base + k
+  unsigned ring_cap;
+  unsigned pool_cap;   // 0: no reuse pool (reclaimed nodes go to `ovf`)
+  // Words freed alone by the current interaction (0 = empty slot).
+  ull fw0, fw1, fw2, fw3;
 
-  HVM_DEV explicit Lane(const Params& p)
-      : P(p), H(p.heap), hb(p.ctrl->heap_bytes), ovf(0), bnext(0), bend(0), allocs(0), net(0), pn(0), fln(0),
-        fwn(0), dirty(false) {
-    for (int k = 0; k < NCOUNT; k++) rw[k] = 0;
-  }
+  HVM_DEV Lane(const Params& p, WarpSmem* w, unsigned ln)
+      : P(p), W(w), ovf(0), bnext(0), bend(0), allocs(0), net(0), lane(ln), ring_base(0), ring_cap(0),
+        pool_cap(POOL), fw0(0), fw1(0), fw2(0), fw3(0) {}
 
   HVM_DEV void fail(int code, ull info) {
     if (atom_cas32(&P.ctrl->error, 0, code) == 0) {
@@ -262,11 +302,11 @@ struct Lane {
   }
 
   HVM_DEV ull* at(ull a) {
-    if (a >= hb) {
+    if (a >= P.heap_bytes) {
       fail(HVM64_ERR_BAD_ADDR, a);
       a = 0;
     }
-    return H + (a >> 3);
+    return P.heap + (a >> 3);
   }
   HVM_DEV ull load(ull a) { return ld_gpu(at(a)); }
   HVM_DEV void store(ull a, ull v) { st_gpu(at(a), v); }
@@ -292,60 +332,78 @@ struct Lane {
   // into both words of every node it hands out and links a node into a
   // free list once both halves are FREE.  Here a node is LOCK-filled when it
   // becomes free (or when its bump chunk is taken) and that fill is fenced
-  // before the node is handed out again, so alloc() itself touches no memory.
-  // A node whose two halves are both freed by the same interaction is
-  // reclaimed without reading the other half.  Otherwise the reference's
+  // before the node is handed out again, so alloc() itself touches no heap
+  // memory.  A node whose two halves are both freed by the same interaction
+  // is reclaimed without reading the other half; otherwise the reference's
   // store-FREE / read-other-half / CAS sequence decides which lane reclaims.
   HVM_DEV void recycle(ull node) {
-    if (fln < FLCAP) {
-      fl[fln++] = node;
-      dirty = true;
+    int k = pool_cap ? atom_add_i32(&W->freed_n, 1) : POOL;
+    if (k < int(pool_cap)) {
+      W->freed[k] = node;
     } else {
       store(node, ovf);  // right word already LOCK
       ovf = node;
     }
   }
-  HVM_DEV void half_free(ull a) {
-    for (int k = 0; k < fwn; k++) {
-      if (fw[k] == (a ^ 8)) {  // both halves freed by this interaction: no one else can claim the node
-        fw[k] = fw[--fwn];
-        ull l = a & ~8ull;
-        store(l, P_LOCK);
-        store(l | 8, P_LOCK);
-        recycle(l);
-        return;
-      }
+  HVM_DEV bool fw_take(ull x) {
+    if (fw0 == x) { fw0 = 0; return true; }
+    if (fw1 == x) { fw1 = 0; return true; }
+    if (fw2 == x) { fw2 = 0; return true; }
+    if (fw3 == x) { fw3 = 0; return true; }
+    return false;
+  }
+  HVM_DEV void fw_add(ull a) {
+    if (!fw0) fw0 = a;
+    else if (!fw1) fw1 = a;
+    else if (!fw2) fw2 = a;
+    else if (!fw3) fw3 = a;
+    else {
+      settle();
+      fw0 = a;
     }
-    store(a, P_FREE);
-    if (load(a ^ 8) == P_FREE) {
+  }
+  HVM_DEV void half_free(ull a) {
+    if (a != 0 && fw_take(a ^ 8)) {  // both halves freed by this interaction: no one else can claim the node
       ull l = a & ~8ull;
-      if (cas(l, P_FREE, P_LOCK) == P_FREE) {
-        // The node may have been reclaimed and reused since the load (ABA):
-        // keep it only if its right word is still free, else hand the left
-        // word back.
-        if (load(l | 8) == P_FREE) {
-          store(l | 8, P_LOCK);
-          recycle(l);
-        } else {
-          store(l, P_FREE);
-        }
-      }
+      store(l, P_LOCK);
+      store(l | 8, P_LOCK);
+      recycle(l);
       return;
     }
-    if (fwn == FWCAP) fwn = 0;
-    fw[fwn++] = a;
+    store(a, P_FREE);
+    fw_add(a);
   }
-  // End of an interaction: later frees of the other halves take the
-  // ordinary path.
-  HVM_DEV void settle() { fwn = 0; }
+  // A word freed alone: a node found fully free is claimed by CAS on its left
+  // word, then kept only if its right word is still free -- between the load
+  // and the CAS the node may have been reclaimed by the other half's owner,
+  // reused, and half-freed again (ABA); then the left word is handed back.
+  HVM_DEV void claim(ull w, ull other) {
+    if (!w || other != P_FREE) return;
+    ull l = w & ~8ull;
+    if (cas(l, P_FREE, P_LOCK) != P_FREE) return;
+    if (load(l | 8) == P_FREE) {
+      store(l | 8, P_LOCK);
+      recycle(l);
+    } else {
+      store(l, P_FREE);
+    }
+  }
+  // End of an interaction: look at the other half of every word freed alone
+  // (the loads are in flight together).
+  HVM_DEV void settle() {
+    ull o0 = fw0 ? load(fw0 ^ 8) : 0, o1 = fw1 ? load(fw1 ^ 8) : 0;
+    ull o2 = fw2 ? load(fw2 ^ 8) : 0, o3 = fw3 ? load(fw3 ^ 8) : 0;
+    claim(fw0, o0);
+    claim(fw1, o1);
+    claim(fw2, o2);
+    claim(fw3, o3);
+    fw0 = fw1 = fw2 = fw3 = 0;
+  }
   HVM_DEV ull alloc() {
     allocs++;
-    if (fln > 0) {
-      if (dirty) {
-        mem_fence();
-        dirty = false;
-      }
-      return fl[--fln];
+    if (pool_cap) {
+      int k = atom_add_i32(&W->pool_n, -1) - 1;
+      if (k >= 0) return W->pool[k];
     }
     if (ovf != 0) {
       ull a = ovf;
@@ -361,7 +419,7 @@ struct Lane {
         fail(HVM64_ERR_OOM, s);
         return 0;
       }
-      lock_fill(H, s, n);
+      lock_fill(P.heap, s, n);
       mem_fence();  // LOCK is visible before any of these nodes escapes
       bnext = s;
       bend = s + n;
@@ -370,16 +428,20 @@ struct Lane {
   }
 
   // ---- redex pushes ----------------------------------------------------------
-  HVM_DEV void overflow();
+  HVM_DEV void overflow_one(ull a, ull b);  // platform driver: ship one redex to shared work
   HVM_DEV void push(ull a, ull b) {
-    if (pn == LBCAP) overflow();
-    pb[2 * pn] = a;
-    pb[2 * pn + 1] = b;
-    pn++;
+    unsigned k = ring_cap ? atom_add_u32(&W->ring_cnt, 1u) : 0u;
+    if (k < ring_cap) {
+      unsigned i = (ring_base + k) & unsigned(SCAP - 1);
+      W->stk[2 * i] = a;
+      W->stk[2 * i + 1] = b;
+    } else {
+      overflow_one(a, b);
+    }
   }
   // linker.rs:70-85
   HVM_DEV void redux(ull a, ull b) {
-    if (skippable(a) && skippable(b)) rw[RW_ERAS]++;
+    if (skippable(a) && skippable(b)) count(&W->rw[RW_ERAS], 1);
     else push(a, b);
   }
 
@@ -497,20 +559,36 @@ struct Lane {
     else link_port_port(a, b);
   }
   HVM_DEV ull trg_target(ull t) { return trg_is_wire(t) ? load(t) : t; }
+  // The target of a Trg about to be consumed by a VM instruction.  A wire is
+  // locked rather than read: every path of the instruction then either frees
+  // that wire or links it at once (which would lock it first), so taking the
+  // lock up front saves a round trip and changes nothing observable.
+  HVM_DEV ull trg_take(ull t) { return trg_is_wire(t) ? lock_target(t) : t; }
+  // link_trg_port for a Trg taken with trg_take (its target already known).
+  HVM_DEV void link_taken(ull t, ull target, ull b) {
+    if (!trg_is_wire(t)) return link_port_port(t, b);
+    if (principal(target) && principal(b)) {
+      half_free(t);
+      redux(target, b);
+    } else {
+      half_link_wire_port(target, t, b);
+      half_link_port_port(b, target);
+    }
+  }
   HVM_DEV void free_trg(ull t) {
     if (trg_is_wire(t)) half_free(t);
   }
 
   // ---- rules (runtime/src/interact.rs) ----------------------------------------
   HVM_DEV void anni2(ull a, ull b) {  // interact.rs:72-79
-    rw[RW_ANNI]++;
+    count(&W->rw[RW_ANNI], 1);
     ull a1 = paddr(a), b1 = paddr(b);
     link_wire_wire(a1, b1);
     link_wire_wire(a1 ^ 8, b1 ^ 8);
   }
   HVM_DEV void comm22(ull a, ull b) {  // interact.rs:118-141
-    rw[RW_COMM]++;
-    rw[EX_COMM22]++;
+    count(&W->rw[RW_COMM], 1);
+    count(&W->rw[EX_COMM22], 1);
     ull a1 = paddr(a), b1 = paddr(b);
     ull A1 = alloc(), A2 = alloc(), B1 = alloc(), B2 = alloc();
     unsigned ta = ptag(a), la = plab(a), tb = ptag(b), lb = plab(b);
@@ -524,13 +602,13 @@ struct Lane {
     link_wire_port(b1 ^ 8, mkport(ta, la, A2));
   }
   HVM_DEV void comm02(ull a, ull b) {  // interact.rs:162-168
-    rw[RW_COMM]++;
+    count(&W->rw[RW_COMM], 1);
     ull b1 = paddr(b);
     link_wire_port(b1, a);
     link_wire_port(b1 ^ 8, a);
   }
   HVM_DEV void switch_num(ull a, ull b) {  // interact.rs:201-223
-    rw[RW_OPER]++;
+    count(&W->rw[RW_OPER], 1);
     ull a1 = paddr(a);
     uint32_t num = uint32_t(b);
     uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
@@ -559,7 +637,7 @@ struct Lane {
     ull a1 = paddr(a);
     ull t1 = load(a1);
     if (ptag(t1) == T_NUM) {
-      rw[RW_OPER]++;
+      count(&W->rw[RW_OPER], 1);
       half_free(a1);
       ull out = binary(uint32_t(b), op, uint32_t(t1));
       link_wire_port(a1 ^ 8, out);
@@ -588,11 +666,11 @@ struct Lane {
   // def.rs:177-189
   HVM_DEV void call(ull port, ull trg) {
     if (ptag(trg) == T_CTR && !def_has(port, plab(trg))) return comm02(port, trg);
-    rw[RW_DREF]++;
+    count(&W->rw[RW_DREF], 1);
     if (port & X_BIT) return expand_call(port, trg);
-    ull before = allocs;
+    unsigned before = allocs;
     run_def(unsigned((paddr(port) >> 3) - 1), trg);
-    rw[EX_DNODES] += allocs - before;
+    count(&W->rw[EX_DNODES], allocs - before);
   }
 
   // ---- interact.rs:6-44 --------------------------------------------------------
@@ -603,7 +681,7 @@ struct Lane {
     if (at == T_REF && bn && !skippable(a)) return call(a, b);
     if (an && bt == T_REF && !skippable(b)) return call(b, a);
     if (an && bn) {
-      rw[RW_ERAS]++;
+      count(&W->rw[RW_ERAS], 1);
       return;
     }
     if (at == T_CTR && bt == T_SWITCH && plab(a) != 0) return comm22(a, b);
@@ -628,21 +706,21 @@ struct Lane {
 
   // ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) ----
   HVM_DEV void do_ctr(unsigned lab, ull trg, ull& o1, ull& o2) {
-    ull port = trg_target(trg);
+    ull port = trg_take(trg);
     if (ptag(port) == T_CTR && plab(port) == lab) {
       free_trg(trg);
-      rw[RW_ANNI]++;
+      count(&W->rw[RW_ANNI], 1);
       o1 = paddr(port);  // Trg::wire
       o2 = paddr(port) ^ 8;
       return;
     }
     ull n = alloc();
-    link_trg_port(trg, mkport(T_CTR, lab, n));
+    link_taken(trg, port, mkport(T_CTR, lab, n));
     o1 = pvar(n);
     o2 = pvar(n ^ 8);
   }
   HVM_DEV void do_op(unsigned op, ull trg, ull& o1, ull& o2) {
-    ull port = trg_target(trg);
+    ull port = trg_take(trg);
     if (ptag(port) == T_NUM) {
       free_trg(trg);
       ull n = alloc();
@@ -657,14 +735,14 @@ struct Lane {
       return;
     }
     ull n = alloc();
-    link_trg_port(trg, mkport(T_OP, op, n));
+    link_taken(trg, port, mkport(T_OP, op, n));
     o1 = pvar(n);
     o2 = pvar(n ^ 8);
   }
   HVM_DEV ull do_op_num(unsigned op, ull trg, uint32_t rhs) {
-    ull port = trg_target(trg);
+    ull port = trg_take(trg);
     if (ptag(port) == T_NUM) {
-      rw[RW_OPER]++;
+      count(&W->rw[RW_OPER], 1);
       free_trg(trg);
       return ull(binary(uint32_t(port), op, rhs));
     }
@@ -673,7 +751,7 @@ struct Lane {
       return P_ERA;
     }
     ull n = alloc();
-    link_trg_port(trg, mkport(T_OP, op, n));
+    link_taken(trg, port, mkport(T_OP, op, n));
     store(n, ull(rhs));
     return pvar(n ^ 8);
   }
@@ -684,9 +762,9 @@ struct Lane {
     return a;
   }
   HVM_DEV void do_switch(ull trg, ull& o1, ull& o2) {
-    ull port = trg_target(trg);
+    ull port = trg_take(trg);
     if (ptag(port) == T_NUM) {
-      rw[RW_OPER]++;
+      count(&W->rw[RW_OPER], 1);
       free_trg(trg);
       uint32_t num = uint32_t(port);
       uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
@@ -706,13 +784,13 @@ struct Lane {
       return;
     }
     if (port == P_ERA) {
-      rw[RW_ERAS]++;
+      count(&W->rw[RW_ERAS], 1);
       free_trg(trg);
       o1 = o2 = P_ERA;
       return;
     }
     ull m = alloc();
-    link_trg_port(trg, mkport(T_SWITCH, 0, m));
+    link_taken(trg, port, mkport(T_SWITCH, 0, m));
     o1 = pvar(m);
     o2 = pvar(m ^ 8);
   }
@@ -720,15 +798,22 @@ struct Lane {
   HVM_DEV void run_def(unsigned id, ull t0) {
     if (id >= P.ndefs) return fail(HVM64_ERR_BAD_INPUT, id);
     const DevDef d = P.defs[id];
-    ull R[MAX_REGS];
+    if (d.nregs <= SMALL_REGS) {
+      exec(d, t0, StridedRegs{W->regs + lane, 32});
+    } else {
+      ull R[MAX_REGS];
+      exec(d, t0, StridedRegs{R, 1});
+    }
+  }
+  HVM_DEV void exec(const DevDef& d, ull t0, StridedRegs R) {
     R[0] = t0;
     const DevInstr* ins = P.instrs + d.ins_off;
     for (unsigned k = 0; k < d.ins_len; k++) {
       const DevInstr I = ins[k];
       switch (I.k) {
         case I_CONST: R[I.a] = I.port; break;
-        case I_LINK: rw[EX_DLINKS]++; link_trg(R[I.a], R[I.b]); break;
-        case I_LINKCONST: rw[EX_DLINKS]++; link_trg_port(R[I.a], I.port); break;
+        case I_LINK: count(&W->rw[EX_DLINKS], 1); link_trg(R[I.a], R[I.b]); break;
+        case I_LINKCONST: count(&W->rw[EX_DLINKS], 1); link_trg_port(R[I.a], I.port); break;
         case I_CTR: {
           ull x, y;
           do_ctr(I.lab, R[I.a], x, y);

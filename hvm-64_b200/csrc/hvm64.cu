@@ -84,20 +84,18 @@ __device__ void q_release(const Params& P, ull pos) {
   st_gpu(&P.q[pos & P.ctrl->q_mask].seq, pos + P.ctrl->q_mask + 1);
 }
 
-// A lane's buffer is full in the middle of an interaction: ship it as one slot.
-__device__ void Lane::overflow() {
+// The warp's stack is full: ship one redex as its own slot (rare: each step
+// starts with HEADROOM free stack slots).
+__device__ void Lane::overflow_one(ull a, ull b) {
   atomicAdd(reinterpret_cast<ull*>(&P.nets[net].pending), 1ull);
   ull pos;
-  if (!q_reserve_push(P, *this, pos, true)) {
-    pn = 0;
-    return;
-  }
+  if (!q_reserve_push(P, *this, pos, true)) return;
   Slot* s = &P.q[pos & P.ctrl->q_mask];
-  st_gpu(reinterpret_cast<ull*>(&s->net), (ull(unsigned(pn)) << 32) | net);
-  for (int k = 0; k < 2 * pn; k++) st_gpu(&s->r[k], pb[k]);
+  st_gpu(reinterpret_cast<ull*>(&s->net), (1ull << 32) | net);
+  st_gpu(&s->r[0], a);
+  st_gpu(&s->r[1], b);
   q_publish(P, pos);
   atomicAdd(&P.ctrl->stat_overflow, 1ull);
-  pn = 0;
 }
 
 __device__ __forceinline__ ull shfl(ull v, int src) { return __shfl_sync(0xffffffffu, v, src); }
@@ -130,39 +128,57 @@ __device__ bool donate(const Params& P, Lane& L, ull* S, unsigned& bot, unsigned
   return true;
 }
 
-// Flush a warp's per-lane counters into its net (warp reduction, one atomic
-// per counter).
-__device__ void flush_counters(const Params& P, Lane& L, int cur) {
+// Flush the warp's counters into its net (one atomic per counter).
+__device__ void flush_counters(const Params& P, WarpSmem& W, int cur) {
   const unsigned lane = threadIdx.x & 31;
-  for (int k = 0; k < NCOUNT; k++) {
-    ull v = L.rw[k];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0 && v) atomicAdd(&P.nets[cur].rw[k], v);
-    L.rw[k] = 0;
+  __syncwarp();
+  if (lane < unsigned(NCOUNT)) {
+    ull v = W.rw[lane];
+    if (v) atomicAdd(&P.nets[cur].rw[lane], v);
+    W.rw[lane] = 0;
   }
+  __syncwarp();
 }
 
-__global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
-  __shared__ ull stk[WARPS][2 * SCAP];
-  __shared__ unsigned stops[WARPS];
+constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
+static_assert(SMEM_BYTES <= 56 * 1024, "four reducer blocks per SM must fit in shared memory");
+
+__global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
-  const unsigned budget0 = unsigned(P.ctrl->lane_budget);
-  ull* S = stk[threadIdx.x >> 5];
+  const unsigned lt = (1u << lane) - 1u, gt = ~lt & ~(1u << lane);
+  ull* S = W.stk;
   Ctrl* C = P.ctrl;
-  Lane L(P);
+  Lane L(P, &W, lane);
+  if (lane < unsigned(NCOUNT)) W.rw[lane] = 0;
+  if (lane == 0) {
+    W.pool_n = 0;
+    W.freed_n = 0;
+    W.ring_cnt = 0;
+    W.st_steps = W.st_lanes = W.st_busy = W.st_idle = 0;
+  }
+  __syncwarp();
   unsigned top = 0, bot = 0;  // warp-uniform ring indices
   int cur = -1;               // the net whose work this warp holds
   bool hungry = false;
   unsigned idle = 0, step = 0;
+  // Deadline from this launch's start (a replayed launch gets a fresh one).
+  const ull deadline = globaltimer() + C->timeout_ns;
+  unsigned nap = 0;  // idle backoff, ns
 
   for (;;) {
-    int err = 0;
-    if (lane == 0) err = ld_gpu32(&C->error);
-    if (__shfl_sync(0xffffffffu, err, 0)) break;
+    // The error word is polled only now and then: every warp reading it each
+    // step would make its L2 line a hot spot.
+    if ((step & 31) == 0) {
+      int err = 0;
+      if (lane == 0) err = ld_gpu32(&C->error);
+      if (__shfl_sync(0xffffffffu, err, 0)) break;
+    }
 
     if (top == bot) {
       if (cur >= 0) {
-        flush_counters(P, L, cur);
+        flush_counters(P, W, cur);
         if (lane == 0) {
           long long old = (long long)atomicAdd(reinterpret_cast<ull*>(&P.nets[cur].pending), ~0ull);
           if (old == 1) atomicAdd(reinterpret_cast<ull*>(&C->nets_left), ~0ull);
@@ -174,20 +190,27 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
       if (lane == 0) got = q_reserve_pop(P, pos) ? 1 : 0;
       got = __shfl_sync(0xffffffffu, got, 0);
       if (!got) {
+        // Idle: back off exponentially (1 us .. 64 us) so that waiting warps
+        // do not crowd the queue's and the counters' L2 lines.
         int stop = 0;
         if (lane == 0) {
           if (!hungry) atomicAdd(reinterpret_cast<ull*>(&C->hungry), 1ull);
           if (ld_gpu64s(&C->nets_left) <= 0) stop = 1;
-          else if ((++idle & 255) == 0 && globaltimer() > C->deadline) {
+          else if ((++idle & 15) == 0 && globaltimer() > deadline) {
             L.fail(HVM64_ERR_TIMEOUT, 1);
             stop = 1;
           }
+          if (ld_gpu32(&C->error)) stop = 1;
         }
         hungry = true;
         if (__shfl_sync(0xffffffffu, stop, 0)) break;
-        __nanosleep(256);
+        nap = nap ? min(nap * 2, 65536u) : 1024u;
+        long long t0 = clock64();
+        __nanosleep(nap);
+        if (lane == 0) W.st_idle += ull(clock64() - t0);
         continue;
       }
+      nap = 0;
       if (hungry && lane == 0) atomicAdd(reinterpret_cast<ull*>(&C->hungry), ~0ull);
       hungry = false;
       idle = 0;
@@ -222,110 +245,176 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(Params P) {
     // A run that never reaches normal form ends at the deadline.
     if ((++step & 1023) == 0) {
       int late = 0;
-      if (lane == 0 && globaltimer() > C->deadline) {
+      if (lane == 0 && globaltimer() > deadline) {
         L.fail(HVM64_ERR_TIMEOUT, 2);
         late = 1;
       }
       if (__shfl_sync(0xffffffffu, late, 0)) break;
     }
 
-    // Take up to 32 redexes off the top, one per lane.  A lane then keeps
-    // reducing: first the newest redex its own interactions made, else one
-    // more from the warp's stack, until its budget for this step is spent.
-    // Nothing is pushed to the stack during the step, so lanes only pop.
-    unsigned n = min(top - bot, 32u);
-    ull a = 0, b = 0;
-    if (lane < n) {
-      unsigned k = (top - n + lane) & (SCAP - 1);
-      a = S[2 * k];
-      b = S[2 * k + 1];
-    }
-    if (lane == 0) stops[threadIdx.x >> 5] = top - n;
-    __syncwarp();
-    if (lane < n) {
-      unsigned budget = budget0;
-      for (;;) {
-        L.interact(a, b);
-        L.settle();
-        if (--budget == 0) break;
-        if (L.pn > 0) {
-          L.pn--;
-          a = L.pb[2 * L.pn];
-          b = L.pb[2 * L.pn + 1];
-          continue;
-        }
-        unsigned old = atomicSub(&stops[threadIdx.x >> 5], 1u);
-        if (int(old - bot) <= 0) break;
-        unsigned k = (old - 1) & (SCAP - 1);
-        a = S[2 * k];
-        b = S[2 * k + 1];
-      }
-    }
-    __syncwarp();
-    {
-      unsigned st = stops[threadIdx.x >> 5];
-      top = int(st - bot) > 0 ? st : bot;
-    }
-    __syncwarp();
-
-    // Append every lane's new redexes.
-    unsigned c = unsigned(L.pn), incl = c;
-    for (int o = 1; o < 32; o <<= 1) {
-      unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= unsigned(o)) incl += v;
-    }
-    unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned pre = incl - c;
-    while ((top - bot) + total > unsigned(SCAP)) {
-      unsigned cnt = min(top - bot, 32u);
-      if (!donate(P, L, S, bot, cnt, cur, true)) break;
+    // Keep HEADROOM slots free for this step's new redexes.
+    while ((top - bot) > unsigned(SCAP - HEADROOM)) {
+      if (!donate(P, L, S, bot, 32u, cur, true)) break;
       if (lane == 0) atomicAdd(&C->stat_spilled, 1ull);
     }
-    for (unsigned k = 0; k < c; k++) {
-      unsigned slot = (top + pre + k) & (SCAP - 1);
-      S[2 * slot] = L.pb[2 * k];
-      S[2 * slot + 1] = L.pb[2 * k + 1];
+
+    // Choose this step's redexes: among the newest 64, the rule class most
+    // common among the newest 32 (ties: the newest); up to 32 of that class
+    // run this step, one per lane, and the others go back on the stack.
+    unsigned w = min(top - bot, 64u);
+    ull a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    bool h0 = lane < w, h1 = lane + 32 < w;
+    if (h0) {
+      unsigned k = (top - 1 - lane) & (SCAP - 1);
+      a0 = S[2 * k];
+      b0 = S[2 * k + 1];
     }
-    L.pn = 0;
-    top += total;
+    if (h1) {
+      unsigned k = (top - 33 - lane) & (SCAP - 1);
+      a1 = S[2 * k];
+      b1 = S[2 * k + 1];
+    }
+    unsigned k0 = h0 ? redex_class(a0, b0) : 0xFFFFFFFFu;
+    unsigned k1 = h1 ? redex_class(a1, b1) : 0xFFFFFFFEu;
+    unsigned peers = __match_any_sync(0xffffffffu, k0);
+    unsigned score = h0 ? ((unsigned(__popc(peers)) << 8) | (255u - lane)) : 0u;
+    unsigned best = __reduce_max_sync(0xffffffffu, score);
+    unsigned key = __shfl_sync(0xffffffffu, k0, int(255u - (best & 255u)));
+    bool s0 = h0 && k0 == key, s1 = h1 && k1 == key;
+    unsigned m0 = __ballot_sync(0xffffffffu, s0), m1 = __ballot_sync(0xffffffffu, s1);
+    unsigned n0 = unsigned(__popc(m0));
+    unsigned r0 = unsigned(__popc(m0 & lt)), r1 = n0 + unsigned(__popc(m1 & lt));
+    bool t1 = s1 && r1 < 32u;
+    bool u0 = h0 && !s0, u1 = h1 && !t1;
+    unsigned um0 = __ballot_sync(0xffffffffu, u0), um1 = __ballot_sync(0xffffffffu, u1);
+    unsigned n = min(n0 + unsigned(__popc(m1)), 32u);
+    unsigned base = top - w;
     __syncwarp();
+    if (s0) {
+      W.sel[2 * r0] = a0;
+      W.sel[2 * r0 + 1] = b0;
+    }
+    if (t1) {
+      W.sel[2 * r1] = a1;
+      W.sel[2 * r1 + 1] = b1;
+    }
+    // Entries that stay keep their relative depth (deeper ones lower).
+    if (u1) {
+      unsigned k = (base + unsigned(__popc(um1 & gt))) & (SCAP - 1);
+      S[2 * k] = a1;
+      S[2 * k + 1] = b1;
+    }
+    if (u0) {
+      unsigned k = (base + unsigned(__popc(um1)) + unsigned(__popc(um0 & gt))) & (SCAP - 1);
+      S[2 * k] = a0;
+      S[2 * k + 1] = b0;
+    }
+    top = base + unsigned(__popc(um0)) + unsigned(__popc(um1));
+    if (lane == 0) W.ring_cnt = 0;
+    long long s0c = clock64();
+    __syncwarp();
+    if (lane < n) {
+      L.ring_base = top;
+      L.ring_cap = unsigned(SCAP) - (top - bot);
+      L.interact(W.sel[2 * lane], W.sel[2 * lane + 1]);
+      L.settle();
+    }
+    __syncwarp();
+    if (lane == 0) {
+      W.st_busy += ull(clock64() - s0c);
+      W.st_lanes += n;
+      W.st_steps++;
+    }
+    {
+      unsigned pushed = min(W.ring_cnt, unsigned(SCAP) - (top - bot));
+      top += pushed;
+    }
+    // Nodes reclaimed in this step become allocatable after a fence.
+    __threadfence();
+    __syncwarp();
+    {
+      int pn = max(W.pool_n, 0);
+      int fn = min(W.freed_n, POOL);
+      int mv = min(fn, POOL - pn);
+      for (int i = int(lane); i < mv; i += 32) W.pool[pn + i] = W.freed[i];
+      for (int i = mv + int(lane); i < fn; i += 32) {
+        // pool full: the rest goes to this lane's overflow list
+        ull node = W.freed[i];
+        L.store(node, L.ovf);
+        L.ovf = node;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        W.pool_n = pn + mv;
+        W.freed_n = 0;
+      }
+      __syncwarp();
+    }
 
     // Share the oldest work when other warps are starving.
-    if (top - bot >= unsigned(C->donate_min) && ((step & 3) == 0)) {
+    if (top - bot >= unsigned(C->donate_min) && ((step & 7) == 0)) {
       int give = 0;
       if (lane == 0) {
         long long h = ld_gpu64s(&C->hungry);
         long long queued = (long long)(ld_gpu(&C->q_tail) - ld_gpu(&C->q_head));
         give = h > 0 && queued < h;
       }
-      if (__shfl_sync(0xffffffffu, give, 0)) {
-        if (donate(P, L, S, bot, 32u, cur, false) && lane == 0) atomicAdd(&C->stat_donated, 1ull);
+      // Give up to half the stack (at most four slots) per check.
+      unsigned chunks = __shfl_sync(0xffffffffu, give, 0) ? min((top - bot) / 64u, 4u) : 0u;
+      for (unsigned k = 0; k < chunks; k++) {
+        if (!donate(P, L, S, bot, 32u, cur, false)) break;
+        if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
       }
     }
   }
-  if (cur >= 0) flush_counters(P, L, cur);
+  if (cur >= 0) flush_counters(P, W, cur);
+  if (lane == 0) {
+    atomicAdd(&C->stat_steps, W.st_steps);
+    atomicAdd(&C->stat_lanes, W.st_lanes);
+    atomicAdd(&C->stat_busy_cycles, W.st_busy);
+    atomicAdd(&C->stat_idle_cycles, W.st_idle);
+  }
 }
 
 // One thread per net: allocate the root, run the boot program against it
 // (Net::boot / Host::encode_net), then wrap the root in an expansion agent
-// (Net::expand, runtime/src/net.rs:65-69).  Redexes go to the global queue.
+// (Net::expand, runtime/src/net.rs:65-69).  Redexes go to the global queue in
+// slots of up to 32.
 __global__ void boot_kernel(Params P, unsigned first, unsigned count) {
   unsigned i = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= first + count) return;
-  Lane L(P);
+  WarpSmem W;  // this thread's private copy (local memory)
+  W.ring_cnt = 0;
+  W.pool_n = W.freed_n = 0;
+  for (int c = 0; c < NCOUNT; c++) W.rw[c] = 0;
+  Lane L(P, &W, 0);
   L.net = i;
+  L.pool_cap = 0;
+  L.ring_base = 0;
+  L.ring_cap = CHUNK;
   NetState& ns = P.nets[i];
   ull root = L.alloc();
   unsigned prog = unsigned(ns.prog);
-  if (prog < P.ndefs && !(P.defs[prog].flags & 1)) L.rw[RW_DREF]++;
+  if (prog < P.ndefs && !(P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
+  // Small Defs use register slots 0, 32, 64, ... of W.regs (lane 0's column).
   L.run_def(prog, pvar(root));
   L.settle();
   root = L.expand(root);
   L.settle();
   ns.root = root;
-  if (L.pn) L.overflow();
-  for (int k = 0; k < NCOUNT; k++)
-    if (L.rw[k]) atomicAdd(&ns.rw[k], L.rw[k]);
+  unsigned k = min(W.ring_cnt, unsigned(CHUNK));
+  if (k) {
+    atomicAdd(reinterpret_cast<ull*>(&ns.pending), 1ull);
+    ull pos;
+    if (q_reserve_push(P, L, pos, true)) {
+      Slot* s = &P.q[pos & P.ctrl->q_mask];
+      st_gpu(reinterpret_cast<ull*>(&s->net), (ull(k) << 32) | i);
+      for (unsigned j = 0; j < 2 * k; j++) st_gpu(&s->r[j], W.stk[j]);
+      q_publish(P, pos);
+    }
+  }
+  for (int c = 0; c < NCOUNT; c++)
+    if (W.rw[c]) atomicAdd(&ns.rw[c], W.rw[c]);
   __threadfence();
   if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&P.ctrl->nets_left), 1ull);
 }
@@ -443,6 +532,7 @@ struct Runner {
   dev::Params params() {
     dev::Params p{};
     p.heap = heap.p;
+    p.heap_bytes = heap_bytes;
     p.ctrl = ctrl.p;
     p.nets = nets.p;
     p.nnets = unsigned(progs.size());
@@ -460,13 +550,16 @@ struct Runner {
     unsigned bt = 128;
     dev::boot_kernel<<<(count + bt - 1) / bt, bt, 0, st>>>(p, first, count);
     CU(cudaGetLastError());
+    CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(dev::SMEM_BYTES)));
     int bps = int(t.blocks_per_sm);
     if (bps <= 0) {
       int occ = 0;
-      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, 0));
+      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS,
+                                                       dev::SMEM_BYTES));
       bps = std::max(1, occ);
     }
-    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, 0, st>>>(p);
+    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>(p);
     CU(cudaGetLastError());
   }
 
@@ -478,10 +571,9 @@ struct Runner {
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
-    c.lane_budget = t.lane_budget ? t.lane_budget : 8;
+    c.lane_budget = t.lane_budget ? t.lane_budget : 1;
     c.q_mask = (1ull << qlog2) - 1;
-    // The deadline is set on the device clock right before launch.
-    c.deadline = ~0ull;
+    c.deadline = ~0ull;  // the boot kernel's deadline; warps of the reducer keep their own
     host_ctrl = c;
     CU(cudaMemcpyAsync(ctrl.p, &c, sizeof c, cudaMemcpyHostToDevice, st));
   }
@@ -505,6 +597,8 @@ struct Runner {
     h2d += host_nets.size() * sizeof(dev::NetState);
 
     stat_donated = stat_spilled = stat_overflow = 0;
+    stat_steps = stat_lanes = stat_busy = stat_idle = 0;
+    for (int k = 0; k < 8; k++) stat_g_steps[k] = stat_g_cycles[k] = 0;
     cudaStream_t st = 0;
     cudaEvent_t e0, e1;
     CU(cudaEventCreate(&e0));
@@ -521,6 +615,8 @@ struct Runner {
       dev::queue_init_kernel<<<unsigned((qn + 255) / 256), 256, 0, st>>>(q.p, qn);
       CU(cudaGetLastError());
       set_deadline(st, timeout_ms);
+      host_ctrl.timeout_ns = timeout_ms * 1000000ull;
+      CU(cudaMemcpyAsync(&ctrl.p->timeout_ns, &host_ctrl.timeout_ns, 8, cudaMemcpyHostToDevice, st));
       CU(cudaEventRecord(e0, st));
       launch(first, count, t, st);
       CU(cudaEventRecord(e1, st));
@@ -534,6 +630,14 @@ struct Runner {
       stat_donated += host_ctrl.stat_donated;
       stat_spilled += host_ctrl.stat_spilled;
       stat_overflow += host_ctrl.stat_overflow;
+      stat_steps += host_ctrl.stat_steps;
+      stat_lanes += host_ctrl.stat_lanes;
+      stat_busy += host_ctrl.stat_busy_cycles;
+      stat_idle += host_ctrl.stat_idle_cycles;
+      for (int k = 0; k < 8; k++) {
+        stat_g_steps[k] += host_ctrl.stat_g_steps[k];
+        stat_g_cycles[k] += host_ctrl.stat_g_cycles[k];
+      }
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
       if (host_ctrl.error) {
         for (unsigned k = first; k < first + count; k++) host_nets[k].status = host_ctrl.error;
@@ -562,6 +666,8 @@ struct Runner {
 
   void set_deadline(cudaStream_t st, uint64_t timeout_ms);
   uint64_t stat_donated = 0, stat_spilled = 0, stat_overflow = 0, heap_used = 0;
+  uint64_t stat_steps = 0, stat_lanes = 0, stat_busy = 0, stat_idle = 0;
+  uint64_t stat_g_steps[8] = {0}, stat_g_cycles[8] = {0};
 
   void stats(hvm64_stats* o) const {
     *o = hvm64_stats{};
@@ -576,6 +682,10 @@ struct Runner {
     o->overflowed = stat_overflow;
     o->h2d_bytes = h2d;
     o->d2h_bytes = d2h;
+    o->steps = stat_steps;
+    o->step_lanes = stat_lanes;
+    o->busy_cycles = stat_busy;
+    o->idle_cycles = stat_idle;
   }
 
   std::string readback(unsigned i) {
@@ -778,6 +888,17 @@ int hvm64_batch_stats(const hvm64_batch* b, hvm64_stats* out) {
   b->r.stats(out);
   return HVM64_OK;
 }
+// Diagnostic (not in the public header): steps and cycles of the last run
+// by the number of distinct rule classes among the lanes of a step.
+int hvm64_internal_class_steps(const hvm64_batch* b, uint64_t* steps8, uint64_t* cycles8) {
+  if (!b) return HVM64_ERR_BAD_INPUT;
+  for (int k = 0; k < 8; k++) {
+    steps8[k] = b->r.stat_g_steps[k];
+    cycles8[k] = b->r.stat_g_cycles[k];
+  }
+  return HVM64_OK;
+}
+
 int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
   if (!n || !out) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
   n->r.stats(out);

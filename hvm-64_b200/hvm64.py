@@ -65,7 +65,8 @@ class Tuning(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("comm22", "dref_nodes", "dref_links", "heap_nodes_used", "donated",
-                                                "spilled", "overflowed", "h2d_bytes", "d2h_bytes")]
+                                                "spilled", "overflowed", "h2d_bytes", "d2h_bytes", "steps",
+                                                "step_lanes", "busy_cycles", "idle_cycles")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

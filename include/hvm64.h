@@ -112,6 +112,8 @@ typedef struct hvm64_stats {
   uint64_t comm22, dref_nodes, dref_links;
   uint64_t heap_nodes_used, donated, spilled, overflowed;
   uint64_t h2d_bytes, d2h_bytes;
+  uint64_t steps, step_lanes;        /* warp steps taken; redexes they started */
+  uint64_t busy_cycles, idle_cycles; /* summed over warps: stepping vs waiting for work */
 } hvm64_stats;
 int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
 int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);

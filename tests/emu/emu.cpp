@@ -12,6 +12,7 @@
 #include <deque>
 #include <mutex>
 #include <string>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -31,38 +32,58 @@ struct Emu {
 };
 thread_local Emu* g_emu = nullptr;
 
-void flush(Lane& L, NetState& ns) {
+void flush(WarpSmem& W, NetState& ns) {
   for (int k = 0; k < NCOUNT; k++) {
-    if (L.rw[k]) atom_add(&ns.rw[k], L.rw[k]);
-    L.rw[k] = 0;
+    if (W.rw[k]) atom_add(&ns.rw[k], W.rw[k]);
+    W.rw[k] = 0;
   }
 }
 
-void worker(Emu* E, unsigned budget, unsigned share_min) {
+// One host thread = one warp of one lane, with the kernel's per-warp state.
+std::unique_ptr<WarpSmem> new_warp() {
+  auto W = std::make_unique<WarpSmem>();
+  memset(W.get(), 0, sizeof(WarpSmem));
+  return W;
+}
+
+void give(Emu* E, WarpSmem& W, unsigned& bot, unsigned cnt, int cur) {
+  std::vector<ull> v;
+  for (unsigned k = 0; k < cnt; k++) {
+    unsigned i = (bot + k) & (SCAP - 1);
+    v.push_back(W.stk[2 * i]);
+    v.push_back(W.stk[2 * i + 1]);
+  }
+  bot += cnt;
+  atom_add(reinterpret_cast<ull*>(&E->nets[cur].pending), 1ull);
+  std::lock_guard<std::mutex> g(E->mu);
+  E->queue.push_back({unsigned(cur), std::move(v)});
+}
+
+void worker(Emu* E, unsigned share_min) {
   g_emu = E;
-  Lane L(E->P);
-  std::vector<ull> st;
+  auto W = new_warp();
+  Lane L(E->P, W.get(), 0);
+  unsigned top = 0, bot = 0;
   int cur = -1;
   for (;;) {
     if (ld_gpu32(&E->C.error)) break;
-    if (st.empty()) {
+    if (top == bot) {
       if (cur >= 0) {
-        flush(L, E->nets[cur]);
+        flush(*W, E->nets[cur]);
         long long old = (long long)atom_add(reinterpret_cast<ull*>(&E->nets[cur].pending), ~0ull);
         if (old == 1) atom_add(reinterpret_cast<ull*>(&E->C.nets_left), ~0ull);
         cur = -1;
       }
-      bool got = false;
+      std::vector<ull> got;
       {
         std::lock_guard<std::mutex> g(E->mu);
         if (!E->queue.empty()) {
           cur = int(E->queue.front().first);
-          st = std::move(E->queue.front().second);
+          got = std::move(E->queue.front().second);
           E->queue.pop_front();
-          got = true;
         }
       }
-      if (!got) {
+      if (cur < 0) {
         if (ld_gpu64s(&E->C.nets_left) <= 0) break;
         if (globaltimer() > E->C.deadline) {
           L.fail(HVM64_ERR_TIMEOUT, 1);
@@ -72,46 +93,48 @@ void worker(Emu* E, unsigned budget, unsigned share_min) {
         continue;
       }
       L.net = unsigned(cur);
+      bot = 0;
+      top = unsigned(got.size() / 2);
+      for (size_t k = 0; k < got.size(); k++) W->stk[k] = got[k];
     }
-    for (unsigned k = 0; k < budget && !st.empty(); k++) {
-      ull b = st.back();
-      st.pop_back();
-      ull a = st.back();
-      st.pop_back();
-      L.interact(a, b);
-      L.settle();
-      for (int i = 0; i < L.pn; i++) {
-        st.push_back(L.pb[2 * i]);
-        st.push_back(L.pb[2 * i + 1]);
-      }
-      L.pn = 0;
+    while (top - bot > unsigned(SCAP - HEADROOM)) give(E, *W, bot, 32, cur);
+    unsigned i = (top - 1) & (SCAP - 1);
+    ull a = W->stk[2 * i], b = W->stk[2 * i + 1];
+    top -= 1;
+    W->ring_cnt = 0;
+    L.ring_base = top;
+    L.ring_cap = unsigned(SCAP) - (top - bot);
+    L.interact(a, b);
+    L.settle();
+    top += std::min(W->ring_cnt, unsigned(SCAP) - (top - bot));
+    // merge reclaimed nodes into the pool
+    int pn = std::max(W->pool_n, 0), fn = std::min(W->freed_n, POOL), mv = std::min(fn, POOL - pn);
+    for (int k = 0; k < mv; k++) W->pool[pn + k] = W->freed[k];
+    for (int k = mv; k < fn; k++) {
+      L.store(W->freed[k], L.ovf);
+      L.ovf = W->freed[k];
     }
-    // Share the oldest half when the queue runs dry.
-    if (st.size() / 2 >= share_min) {
-      std::lock_guard<std::mutex> g(E->mu);
-      if (E->queue.size() < 4) {
-        size_t half = (st.size() / 4) * 2;
-        std::vector<ull> give(st.begin(), st.begin() + long(half));
-        st.erase(st.begin(), st.begin() + long(half));
-        atom_add(reinterpret_cast<ull*>(&E->nets[cur].pending), 1ull);
-        E->queue.push_back({unsigned(cur), std::move(give)});
+    W->pool_n = pn + mv;
+    W->freed_n = 0;
+    if (top - bot >= share_min) {
+      bool want;
+      {
+        std::lock_guard<std::mutex> g(E->mu);
+        want = E->queue.size() < 4;
       }
+      if (want) give(E, *W, bot, std::min(32u, (top - bot) / 2), cur);
     }
   }
-  if (cur >= 0) flush(L, E->nets[cur]);
+  if (cur >= 0) flush(*W, E->nets[cur]);
 }
 }  // namespace
 
-// The emulation ships a full lane buffer to the shared queue.
-void hvm::dev::Lane::overflow() {
+// The emulation ships an overflowing redex to the shared queue.
+void hvm::dev::Lane::overflow_one(ull a, ull b) {
   Emu* E = g_emu;
   atom_add(reinterpret_cast<ull*>(&P.nets[net].pending), 1ull);
-  std::vector<ull> v(pb, pb + 2 * pn);
-  {
-    std::lock_guard<std::mutex> g(E->mu);
-    E->queue.push_back({net, std::move(v)});
-  }
-  pn = 0;
+  std::lock_guard<std::mutex> g(E->mu);
+  E->queue.push_back({net, std::vector<ull>{a, b}});
 }
 
 extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned threads, unsigned budget,
@@ -134,6 +157,7 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     E.C.spin_limit = 1ull << 26;
     E.C.deadline = globaltimer() + 120ull * 1000000000ull;
     E.P.heap = E.heap.data();
+    E.P.heap_bytes = heap_bytes;
     E.P.ctrl = &E.C;
     E.P.nets = E.nets.data();
     E.P.nnets = 1;
@@ -144,21 +168,23 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     // boot (the boot kernel's steps, one thread)
     g_emu = &E;
     {
-      Lane L(E.P);
+      auto W = new_warp();
+      Lane L(E.P, W.get(), 0);
+      L.ring_cap = 0;  // boot redexes go straight to the shared queue
       L.net = 0;
       ull root = L.alloc();
-      if (!(book.defs[it->second].flags & 1)) L.rw[RW_DREF]++;
+      if (!(book.defs[it->second].flags & 1)) W->rw[RW_DREF]++;
       L.run_def(it->second, pvar(root));
       L.settle();
       root = L.expand(root);
       L.settle();
       E.nets[0].root = root;
-      if (L.pn) L.overflow();
-      flush(L, E.nets[0]);
+      flush(*W, E.nets[0]);
       if (E.nets[0].pending > 0) E.C.nets_left = 1;
     }
+    (void)budget;
     std::vector<std::thread> th;
-    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, budget, share_min);
+    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min);
     for (auto& t : th) t.join();
     if (E.C.error) {
       snprintf(err, errcap, "device error %d info 0x%llx", E.C.error, (unsigned long long)E.C.error_info);
