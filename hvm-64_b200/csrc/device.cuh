@@ -36,11 +36,12 @@ typedef unsigned long long ull;
 
 constexpr int WARPS = 4;            // warps per reducer block
 constexpr int THREADS = WARPS * 32;
-constexpr int SCAP = 512;           // per-warp shared-memory redex stack (power of two)
-constexpr int HEADROOM = 192;       // stack slots kept free for the redexes of one step
+constexpr int SCAP = 256;           // per-warp shared-memory redex stack (power of two)
+constexpr int HEADROOM = 128;       // stack slots kept free for the redexes of one step
 constexpr int CHUNK = 32;           // redexes per global-queue slot
-constexpr int POOL = 128;           // per-warp pool of free nodes ready for reuse
-constexpr unsigned SMALL_REGS = 12; // Defs with at most this many registers use shared memory
+constexpr int POOL = 64;            // per-warp pool of free nodes ready for reuse
+constexpr unsigned ICACHE = 32;     // instructions of the step's Def staged in shared memory
+constexpr unsigned SMALL_REGS = 10; // Defs with at most this many registers use shared memory
 
 constexpr ull P_ERA = 2;
 constexpr ull P_FREE = 0x8000000000000000ull;
@@ -77,7 +78,8 @@ struct Ctrl {
   ull stat_donated, stat_spilled, stat_overflow, stat_taken;
   ull stat_steps, stat_lanes, stat_busy_cycles, stat_idle_cycles;
   ull timeout_ns;  // per launch: each warp's deadline is its start + timeout_ns
-  ull stat_g_steps[8], stat_g_cycles[8];  // steps by number of distinct rule classes among lanes
+  ull stat_lane_sum, stat_lane_max, stat_total;  // per-lane interaction cycles (sum, per-step max), warp lifetime
+  ull stat_prof[8];  // profiling build: loads, exchanges, CAS (count, cycles), stores
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -112,6 +114,14 @@ struct Params {
   unsigned ndefs;
 };
 
+// The run's parameters: CUDA constant memory (set before each launch), or a
+// plain global in the host emulation.
+#ifdef __CUDACC__
+__constant__ Params g_P;
+#else
+inline Params g_P;
+#endif
+
 // ---- platform layer ------------------------------------------------------------
 // The runtime below is written against these few operations.  Under nvcc
 // they are strong GPU-scope PTX accesses and CUDA atomics; under a host
@@ -121,6 +131,9 @@ struct Params {
 #ifdef __CUDACC__
 #define HVM_DEV __device__
 #define HVM_INL __device__ __forceinline__
+// Rare paths stay out of line so the hot loop stays small (instruction cache)
+// and needs fewer registers.
+#define HVM_COLD __device__ __noinline__
 __device__ __forceinline__ ull ld_gpu(const ull* p) {
   ull v;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -145,7 +158,9 @@ __device__ __forceinline__ ull atom_add(ull* p, ull v) { return atomicAdd(p, v);
 __device__ __forceinline__ int atom_cas32(int* p, int e, int v) { return atomicCAS(p, e, v); }
 __device__ __forceinline__ unsigned atom_add_u32(unsigned* p, unsigned v) { return atomicAdd(p, v); }
 __device__ __forceinline__ int atom_add_i32(int* p, int v) { return atomicAdd(p, v); }
-__device__ __forceinline__ void mem_fence() { __threadfence(); }
+// A release fence: the node fills and links before it are visible to any
+// lane that later reaches the node through a port published after it.
+__device__ __forceinline__ void mem_fence() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void pause_brief() { __nanosleep(64); }
 // LOCK-fill nodes [s, s+n) with 16-byte stores.
 __device__ __forceinline__ void lock_fill(ull* H, ull s, ull n) {
@@ -155,6 +170,7 @@ __device__ __forceinline__ void lock_fill(ull* H, ull s, ull n) {
 #else
 #define HVM_DEV
 #define HVM_INL inline
+#define HVM_COLD __attribute__((noinline))
 #ifdef HVM_EMU_STRESS
 // Test builds only: yield at random inside memory operations to widen race
 // windows.
@@ -234,14 +250,6 @@ HVM_INL unsigned redex_class(ull a, ull b) {
   return 16 + at * 8 + bt;      // commutation / native ops
 }
 
-// VM register files: a warp's shared-memory block laid out [register][lane],
-// or a local array for the rare Def needing more than SMALL_REGS.
-struct StridedRegs {
-  ull* base;
-  unsigned stride;
-  HVM_INL ull& operator[](unsigned i) const { return base[i * stride]; }
-};
-
 // Per-warp shared state of the reducer (one per warp; the CPU emulation
 // harness gives each host thread one too).
 struct WarpSmem {
@@ -250,648 +258,682 @@ struct WarpSmem {
   ull pool[POOL];             // free nodes ready for reuse
   ull freed[POOL];            // nodes reclaimed during the current step
   ull sel[64];                // the redexes chosen for the current step
+  DevInstr icache[ICACHE];    // the instructions of `icache_def`, staged for this step
+  DevDef idef;                // that Def's header
+  unsigned icache_def;        // Def index staged in icache (~0u: none)
   ull rw[NCOUNT];             // counters of the warp's current net
-  ull st_steps, st_lanes, st_busy, st_idle;
+  ull ovf[32];                // per lane: overflow free list (left word links; right word LOCK)
+  ull fw[4 * 32];             // per lane: words freed alone by the current interaction
+  ull bnext[32], bend[32];    // per lane: pre-LOCKed bump chunk [bnext, bend), node indices
+  unsigned allocs[32];        // per lane: nodes allocated (for the DREF statistics)
+  unsigned ring_base;         // this step's pushes go to stack slots ring_base + k ...
+  unsigned ring_cap;          // ... for k < ring_cap
+  int pool_cap;               // 0: no reuse pool (reclaimed nodes go to `ovf`)
+#ifdef HVM_PROFILE_OPS
+  ull prof[8];                // profiling build: op counts and wait cycles
+#endif
+  ull st_steps, st_lanes, st_busy, st_idle, st_lane_sum, st_lane_max, st_total;
   unsigned ring_cnt;
   int pool_n;
   int freed_n;
   unsigned pad;
 };
 
-HVM_INL void count(ull* c, ull v) { atom_add(c, v); }
+// Initial per-lane / per-warp runtime state (lane `ln` of warp state `W`).
+HVM_INL void lane_init(WarpSmem* W, unsigned ln) {
+  W->ovf[ln] = 0;
+  for (int k = 0; k < 4; k++) W->fw[k * 32 + ln] = 0;
+  W->bnext[ln] = W->bend[ln] = 0;
+  W->allocs[ln] = 0;
+}
 
-struct Lane {
-  const Params& P;
-  WarpSmem* W;      // this lane's warp state (sinks, pools, counters, VM registers)
-  ull ovf;          // overflow free list (left word links; right word LOCK)
-  ull bnext;        // pre-LOCKed bump chunk [bnext, bend) in node indices
-  ull bend;
-  unsigned allocs;  // nodes allocated by this lane (for the DREF statistics)
-  unsigned net;
+// ---- cold paths as free functions over scalars -------------------------------
+// (A Lane never has its address taken, so its state stays in registers.)
+HVM_COLD void run_fail(unsigned net, int code, ull info) {
+  if (atom_cas32(&g_P.ctrl->error, 0, code) == 0) {
+    g_P.ctrl->error_info = info;
+    g_P.ctrl->error_net = int(net);
+  }
+}
+HVM_INL bool run_failed() { return ld_gpu32(&g_P.ctrl->error) != 0; }
+// One poll of a bounded wait; false = abandon the wait.
+HVM_INL bool run_spin(unsigned net, unsigned& it) {
+  ++it;
+  if ((it & 63) == 0) {
+    if (run_failed()) return false;
+    if (it > g_P.ctrl->spin_limit) {
+      run_fail(net, HVM64_ERR_TIMEOUT, 0);
+      return false;
+    }
+    pause_brief();
+  }
+  return true;
+}
+HVM_INL ull* heap_at(unsigned net, ull a) {
+  if (a >= g_P.heap_bytes) {
+    run_fail(net, HVM64_ERR_BAD_ADDR, a);
+    a = 0;
+  }
+  return g_P.heap + (a >> 3);
+}
+// wire.rs:342-350: wait until the word is not LOCK and take it.
+HVM_COLD ull relock(unsigned net, ull w) {
+  unsigned it = 0;
+  for (;;) {
+    ull got = atom_exch(heap_at(net, w), P_LOCK);
+    if (got != P_LOCK) return got;
+    if (!run_spin(net, it)) return P_ERA;
+  }
+}
+HVM_COLD uint32_t binary_op(unsigned net, uint32_t a, uint32_t op, uint32_t b) {
+  int e = 0;
+  uint32_t r = num_binary(a, op, b, &e);
+  if (e) run_fail(net, HVM64_ERR_DIV0, net);
+  return r;
+}
+// The warp's stack had no room: the platform driver ships the redex to
+// shared work (the CUDA driver: a one-redex queue slot).
+HVM_COLD void push_overflow(unsigned net, ull a, ull b);
+// Pop the rare overflow free list / take a new pre-LOCKed bump chunk.
+struct Refill {
+  ull node, bnext, bend;
+};
+HVM_COLD Refill alloc_refill(unsigned net, ull* ovf) {
+  if (*ovf != 0) {
+    ull a = *ovf;
+    *ovf = ld_gpu(heap_at(net, a));
+    st_gpu(heap_at(net, a), P_LOCK);
+    mem_fence();
+    return {a, 0, 0};
+  }
+  ull n = g_P.ctrl->chunk_nodes;
+  ull s = atom_add(&g_P.ctrl->bump, n);
+  if (s + n > g_P.ctrl->heap_nodes) {
+    run_fail(net, HVM64_ERR_OOM, s);
+    return {0, 0, 0};
+  }
+  lock_fill(g_P.heap, s, n);
+  mem_fence();  // LOCK is visible before any of these nodes escapes
+  return {s << 4, s + 1, s + n};
+}
+
+// ---- the runtime proper ------------------------------------------------------
+// Every rule, link operation and VM instruction is one out-of-line function
+// over a three-word context (warp state, lane, net).  A lane's mutable state
+// (freed-word slots, bump chunk) lives in its warp's shared memory, so these
+// functions keep nothing in local memory and each exists once in the binary:
+// the hot code fits the instruction cache.
+struct Ctx {
+  WarpSmem* W;
   unsigned lane;
-  unsigned ring_base;  // this step's pushes go to stack slots ring_base + k
-  unsigned ring_cap;
-  unsigned pool_cap;   // 0: no reuse pool (reclaimed nodes go to `ovf`)
-  // Words freed alone by the current interaction (0 = empty slot).
-  ull fw0, fw1, fw2, fw3;
+  unsigned net;
+};
 
-  HVM_DEV Lane(const Params& p, WarpSmem* w, unsigned ln)
-      : P(p), W(w), ovf(0), bnext(0), bend(0), allocs(0), net(0), lane(ln), ring_base(0), ring_cap(0),
-        pool_cap(POOL), fw0(0), fw1(0), fw2(0), fw3(0) {}
+#define LS(field) (c.W->field[c.lane])             // a lane's slot
+#define FW(k) (c.W->fw[(k) * 32 + c.lane])          // freed-word slot k
 
-  HVM_DEV void fail(int code, ull info) {
-    if (atom_cas32(&P.ctrl->error, 0, code) == 0) {
-      P.ctrl->error_info = info;
-      P.ctrl->error_net = int(net);
-    }
-  }
-  HVM_DEV bool failed() const { return ld_gpu32(&P.ctrl->error) != 0; }
+HVM_INL ull hload(const Ctx& c, ull a) {
+#if defined(HVM_PROFILE_OPS) && defined(__CUDACC__)
+  long long t = clock64();
+  ull v = ld_gpu(heap_at(c.net, a));
+  asm volatile("" : "+l"(v));
+  atomicAdd(&c.W->prof[0], 1ull);
+  atomicAdd(&c.W->prof[1], ull(clock64() - t));
+  return v;
+#else
+  return ld_gpu(heap_at(c.net, a));
+#endif
+}
+HVM_INL void hstore(const Ctx& c, ull a, ull v) { st_gpu(heap_at(c.net, a), v); }
+HVM_INL ull hswap(const Ctx& c, ull a, ull v) { return atom_exch(heap_at(c.net, a), v); }
+HVM_INL ull hcas(const Ctx& c, ull a, ull e, ull v) { return atom_cas(heap_at(c.net, a), e, v); }
+HVM_INL void count(const Ctx& c, int k, ull v = 1) { atom_add(&c.W->rw[k], v); }
 
-  // One poll of a bounded wait; false = abandon the wait.
-  HVM_DEV bool spin(unsigned& it) {
-    ++it;
-    if ((it & 63) == 0) {
-      if (failed()) return false;
-      if (it > P.ctrl->spin_limit) {
-        fail(HVM64_ERR_TIMEOUT, 0);
-        return false;
-      }
-      pause_brief();
-    }
-    return true;
-  }
+// wire.rs:342-350
+HVM_INL ull lock_target(const Ctx& c, ull w) {
+  ull got = hswap(c, w, P_LOCK);
+  return got != P_LOCK ? got : relock(c.net, w);
+}
 
-  HVM_DEV ull* at(ull a) {
-    if (a >= P.heap_bytes) {
-      fail(HVM64_ERR_BAD_ADDR, a);
-      a = 0;
-    }
-    return P.heap + (a >> 3);
+// ---- allocator -------------------------------------------------------------
+// The reference's allocator (runtime/src/allocator.rs:73-110) writes LOCK
+// into both words of every node it hands out and links a node into a free
+// list once both halves are FREE.  Here a node is LOCK-filled when it becomes
+// free (or when its bump chunk is taken) and that fill is fenced before the
+// node is handed out again, so alloc() itself touches no heap memory.  A node
+// whose two halves are both freed by the same interaction is reclaimed
+// without reading the other half; otherwise the reference's store-FREE /
+// read-other-half / CAS sequence decides which lane reclaims.
+HVM_COLD void recycle(const Ctx& c, ull node) {
+  int k = c.W->pool_cap ? atom_add_i32(&c.W->freed_n, 1) : POOL;
+  if (k < c.W->pool_cap) {
+    c.W->freed[k] = node;
+  } else {
+    hstore(c, node, LS(ovf));  // right word already LOCK
+    LS(ovf) = node;
   }
-  HVM_DEV ull load(ull a) { return ld_gpu(at(a)); }
-  HVM_DEV void store(ull a, ull v) { st_gpu(at(a), v); }
-  HVM_DEV ull swap(ull a, ull v) { return atom_exch(at(a), v); }
-  HVM_DEV ull cas(ull a, ull e, ull v) { return atom_cas(at(a), e, v); }
+}
+HVM_COLD ull alloc_slow(const Ctx& c) {
+  Refill r = alloc_refill(c.net, &LS(ovf));
+  if (r.bend) {
+    LS(bnext) = r.bnext;
+    LS(bend) = r.bend;
+  }
+  return r.node;
+}
+HVM_INL ull alloc(const Ctx& c) {
+  LS(allocs)++;
+  if (c.W->pool_cap) {
+    int k = atom_add_i32(&c.W->pool_n, -1) - 1;
+    if (k >= 0) return c.W->pool[k];
+  }
+  ull b = LS(bnext);
+  if (b != LS(bend)) {
+    LS(bnext) = b + 1;
+    return b << 4;
+  }
+  return alloc_slow(c);
+}
+// A word freed alone: a node found fully free is claimed by CAS on its left
+// word, then kept only if its right word is still free -- between the load
+// and the CAS the node may have been reclaimed by the other half's owner,
+// reused, and half-freed again (ABA); then the left word is handed back.
+HVM_COLD void claim(const Ctx& c, ull w, ull other) {
+  if (!w || other != P_FREE) return;
+  ull l = w & ~8ull;
+  if (hcas(c, l, P_FREE, P_LOCK) != P_FREE) return;
+  if (hload(c, l | 8) == P_FREE) {
+    hstore(c, l | 8, P_LOCK);
+    recycle(c, l);
+  } else {
+    hstore(c, l, P_FREE);
+  }
+}
+// End of an interaction: look at the other half of every word freed alone
+// (the loads are in flight together).
+HVM_COLD void settle(const Ctx& c) {
+  ull w0 = FW(0), w1 = FW(1), w2 = FW(2), w3 = FW(3);
+  if (!(w0 | w1 | w2 | w3)) return;
+  ull o0 = w0 ? hload(c, w0 ^ 8) : 0, o1 = w1 ? hload(c, w1 ^ 8) : 0;
+  ull o2 = w2 ? hload(c, w2 ^ 8) : 0, o3 = w3 ? hload(c, w3 ^ 8) : 0;
+  FW(0) = FW(1) = FW(2) = FW(3) = 0;
+  claim(c, w0, o0);
+  claim(c, w1, o1);
+  claim(c, w2, o2);
+  claim(c, w3, o3);
+}
+HVM_COLD void half_free(const Ctx& c, ull a) {
+  ull x = a ^ 8;
+  int k = -1;
+  if (a != 0) {
+    if (FW(0) == x) k = 0;
+    else if (FW(1) == x) k = 1;
+    else if (FW(2) == x) k = 2;
+    else if (FW(3) == x) k = 3;
+  }
+  if (k >= 0) {  // both halves freed by this interaction: no one else can claim the node
+    FW(k) = 0;
+    ull l = a & ~8ull;
+    hstore(c, l, P_LOCK);
+    hstore(c, l | 8, P_LOCK);
+    recycle(c, l);
+    return;
+  }
+  hstore(c, a, P_FREE);
+  if (FW(0) == 0) FW(0) = a;
+  else if (FW(1) == 0) FW(1) = a;
+  else if (FW(2) == 0) FW(2) = a;
+  else if (FW(3) == 0) FW(3) = a;
+  else {
+    settle(c);
+    FW(0) = a;
+  }
+}
 
-  // wire.rs:342-350
-  HVM_DEV ull relock(ull w) {
-    unsigned it = 0;
-    for (;;) {
-      ull got = swap(w, P_LOCK);
-      if (got != P_LOCK) return got;
-      if (!spin(it)) return P_ERA;
-    }
+// ---- redex pushes (linker.rs:70-85) -----------------------------------------
+HVM_INL void push(const Ctx& c, ull a, ull b) {
+  unsigned cap = c.W->ring_cap;
+  unsigned k = cap ? atom_add_u32(&c.W->ring_cnt, 1u) : 0u;
+  if (k < cap) {
+    unsigned i = (c.W->ring_base + k) & unsigned(SCAP - 1);
+    c.W->stk[2 * i] = a;
+    c.W->stk[2 * i + 1] = b;
+  } else {
+    push_overflow(c.net, a, b);
   }
-  HVM_DEV ull lock_target(ull w) {
-    ull got = swap(w, P_LOCK);
-    return got != P_LOCK ? got : relock(w);
-  }
+}
+HVM_INL void redux(const Ctx& c, ull a, ull b) {
+  if (skippable(a) && skippable(b)) count(c, RW_ERAS);
+  else push(c, a, b);
+}
 
-  // ---- allocator -------------------------------------------------------------
-  // The reference's allocator (runtime/src/allocator.rs:73-110) writes LOCK
-  // into both words of every node it hands out and links a node into a
-  // free list once both halves are FREE.  Here a node is LOCK-filled when it
-  // becomes free (or when its bump chunk is taken) and that fill is fenced
-  // before the node is handed out again, so alloc() itself touches no heap
-  // memory.  A node whose two halves are both freed by the same interaction
-  // is reclaimed without reading the other half; otherwise the reference's
-  // store-FREE / read-other-half / CAS sequence decides which lane reclaims.
-  HVM_DEV void recycle(ull node) {
-    int k = pool_cap ? atom_add_i32(&W->freed_n, 1) : POOL;
-    if (k < int(pool_cap)) {
-      W->freed[k] = node;
-    } else {
-      store(node, ovf);  // right word already LOCK
-      ovf = node;
+// ---- linker (runtime/src/linker.rs:25-203) ----------------------------------
+HVM_INL void half_link_port_port(const Ctx& c, ull a, ull b) {
+  if (ptag(a) == T_VAR) hstore(c, paddr(a), b);
+}
+HVM_INL void link_port_port(const Ctx& c, ull a, ull b) {
+  if (principal(a) && principal(b)) {
+    redux(c, a, b);
+  } else {
+    half_link_port_port(c, a, b);
+    half_link_port_port(c, b, a);
+  }
+}
+HVM_COLD void resolve_redirect_pri(const Ctx& c, ull ap, ull aw, ull bp);
+// The CAS lost against another lane linking the same wire: leave a redirect
+// (linker.rs:109-123).
+HVM_COLD void half_link_failed(const Ctx& c, ull ap, ull aw, ull bp) {
+  if (ptag(bp) == T_VAR) {
+    hstore(c, aw, pred(paddr(bp)));
+  } else if (principal(bp)) {
+    hstore(c, aw, bp);
+    resolve_redirect_pri(c, ap, aw, bp);
+  } else {
+    run_fail(c.net, HVM64_ERR_BAD_PAIR, bp);
+  }
+}
+HVM_COLD void half_link_wire_port(const Ctx& c, ull ap, ull aw, ull bp) {
+  if (ptag(ap) == T_VAR) {
+    if (hcas(c, paddr(ap), pvar(aw), bp) == pvar(aw)) half_free(c, aw);
+    else half_link_failed(c, ap, aw, bp);
+  } else {
+    half_free(c, aw);
+  }
+}
+HVM_COLD void link_wire_wire(const Ctx& c, ull aw, ull bw) {
+  ull ap = lock_target(c, aw);
+  ull bp = lock_target(c, bw);
+  if (principal(ap) && principal(bp)) {
+    half_free(c, aw);
+    half_free(c, bw);
+    redux(c, ap, bp);
+  } else {
+    half_link_wire_port(c, ap, aw, bp);
+    half_link_wire_port(c, bp, bw, ap);
+  }
+}
+// link_wire_port for a wire whose target `ap` was already taken (locked).
+HVM_COLD void link_locked_wire_port(const Ctx& c, ull aw, ull ap, ull bp) {
+  if (principal(ap) && principal(bp)) {
+    half_free(c, aw);
+    redux(c, ap, bp);
+  } else {
+    half_link_wire_port(c, ap, aw, bp);
+    half_link_port_port(c, bp, ap);
+  }
+}
+HVM_INL void link_wire_port(const Ctx& c, ull aw, ull bp) { link_locked_wire_port(c, aw, lock_target(c, aw), bp); }
+HVM_COLD void resolve_redirect_pri(const Ctx& c, ull ap, ull aw, ull bp) {
+  unsigned it = 0;
+  for (;;) {
+    ull tw = paddr(ap);
+    ull tp = hload(c, tw);
+    if (tp == P_LOCK) {
+      if (!run_spin(c.net, it)) return;
+      continue;
     }
-  }
-  HVM_DEV bool fw_take(ull x) {
-    if (fw0 == x) { fw0 = 0; return true; }
-    if (fw1 == x) { fw1 = 0; return true; }
-    if (fw2 == x) { fw2 = 0; return true; }
-    if (fw3 == x) { fw3 = 0; return true; }
-    return false;
-  }
-  HVM_DEV void fw_add(ull a) {
-    if (!fw0) fw0 = a;
-    else if (!fw1) fw1 = a;
-    else if (!fw2) fw2 = a;
-    else if (!fw3) fw3 = a;
-    else {
-      settle();
-      fw0 = a;
+    if (ptag(tp) == T_RED) {
+      half_free(c, tw);
+      ap = tp;
+      continue;
     }
-  }
-  HVM_DEV void half_free(ull a) {
-    if (a != 0 && fw_take(a ^ 8)) {  // both halves freed by this interaction: no one else can claim the node
-      ull l = a & ~8ull;
-      store(l, P_LOCK);
-      store(l | 8, P_LOCK);
-      recycle(l);
-      return;
-    }
-    store(a, P_FREE);
-    fw_add(a);
-  }
-  // A word freed alone: a node found fully free is claimed by CAS on its left
-  // word, then kept only if its right word is still free -- between the load
-  // and the CAS the node may have been reclaimed by the other half's owner,
-  // reused, and half-freed again (ABA); then the left word is handed back.
-  HVM_DEV void claim(ull w, ull other) {
-    if (!w || other != P_FREE) return;
-    ull l = w & ~8ull;
-    if (cas(l, P_FREE, P_LOCK) != P_FREE) return;
-    if (load(l | 8) == P_FREE) {
-      store(l | 8, P_LOCK);
-      recycle(l);
-    } else {
-      store(l, P_FREE);
-    }
-  }
-  // End of an interaction: look at the other half of every word freed alone
-  // (the loads are in flight together).
-  HVM_DEV void settle() {
-    ull o0 = fw0 ? load(fw0 ^ 8) : 0, o1 = fw1 ? load(fw1 ^ 8) : 0;
-    ull o2 = fw2 ? load(fw2 ^ 8) : 0, o3 = fw3 ? load(fw3 ^ 8) : 0;
-    claim(fw0, o0);
-    claim(fw1, o1);
-    claim(fw2, o2);
-    claim(fw3, o3);
-    fw0 = fw1 = fw2 = fw3 = 0;
-  }
-  HVM_DEV ull alloc() {
-    allocs++;
-    if (pool_cap) {
-      int k = atom_add_i32(&W->pool_n, -1) - 1;
-      if (k >= 0) return W->pool[k];
-    }
-    if (ovf != 0) {
-      ull a = ovf;
-      ovf = load(a);
-      store(a, P_LOCK);
-      mem_fence();
-      return a;
-    }
-    if (bnext == bend) {
-      ull n = P.ctrl->chunk_nodes;
-      ull s = atom_add(&P.ctrl->bump, n);
-      if (s + n > P.ctrl->heap_nodes) {
-        fail(HVM64_ERR_OOM, s);
-        return 0;
-      }
-      lock_fill(P.heap, s, n);
-      mem_fence();  // LOCK is visible before any of these nodes escapes
-      bnext = s;
-      bend = s + n;
-    }
-    return (bnext++) << 4;
-  }
-
-  // ---- redex pushes ----------------------------------------------------------
-  HVM_DEV void overflow_one(ull a, ull b);  // platform driver: ship one redex to shared work
-  HVM_DEV void push(ull a, ull b) {
-    unsigned k = ring_cap ? atom_add_u32(&W->ring_cnt, 1u) : 0u;
-    if (k < ring_cap) {
-      unsigned i = (ring_base + k) & unsigned(SCAP - 1);
-      W->stk[2 * i] = a;
-      W->stk[2 * i + 1] = b;
-    } else {
-      overflow_one(a, b);
-    }
-  }
-  // linker.rs:70-85
-  HVM_DEV void redux(ull a, ull b) {
-    if (skippable(a) && skippable(b)) count(&W->rw[RW_ERAS], 1);
-    else push(a, b);
-  }
-
-  // ---- linker (runtime/src/linker.rs:25-203) --------------------------------
-  HVM_DEV void half_link_port_port(ull a, ull b) {
-    if (ptag(a) == T_VAR) store(paddr(a), b);
-  }
-  HVM_DEV void link_port_port(ull a, ull b) {
-    if (principal(a) && principal(b)) {
-      redux(a, b);
-    } else {
-      half_link_port_port(a, b);
-      half_link_port_port(b, a);
-    }
-  }
-  HVM_DEV void link_wire_wire(ull aw, ull bw) {
-    // Lock order as in the reference: a lane waiting on `aw` must not hold
-    // `bw`, or a lane resolving a redirect through `bw` could wait on it.
-    ull ap = lock_target(aw);
-    ull bp = lock_target(bw);
-    if (principal(ap) && principal(bp)) {
-      half_free(aw);
-      half_free(bw);
-      redux(ap, bp);
-    } else {
-      half_link_wire_port(ap, aw, bp);
-      half_link_wire_port(bp, bw, ap);
-    }
-  }
-  HVM_DEV void link_wire_port(ull aw, ull bp) {
-    ull ap = lock_target(aw);
-    if (principal(ap) && principal(bp)) {
-      half_free(aw);
-      redux(ap, bp);
-    } else {
-      half_link_wire_port(ap, aw, bp);
-      half_link_port_port(bp, ap);
-    }
-  }
-  HVM_DEV void half_link_wire_port(ull ap, ull aw, ull bp) {
-    if (ptag(ap) == T_VAR) {
-      if (cas(paddr(ap), pvar(aw), bp) == pvar(aw)) {
-        half_free(aw);
-      } else if (ptag(bp) == T_VAR) {
-        store(aw, pred(paddr(bp)));
-      } else if (principal(bp)) {
-        store(aw, bp);
-        resolve_redirect_pri(ap, aw, bp);
-      } else {
-        fail(HVM64_ERR_BAD_PAIR, bp);
-      }
-    } else {
-      half_free(aw);
-    }
-  }
-  HVM_DEV void resolve_redirect_pri(ull ap, ull aw, ull bp) {
-    unsigned it = 0;
-    for (;;) {
-      ull tw = paddr(ap);
-      ull tp = load(tw);
-      if (tp == P_LOCK) {
-        if (!spin(it)) return;
-        continue;
-      }
-      if (ptag(tp) == T_RED) {
-        half_free(tw);
-        ap = tp;
-        continue;
-      }
-      if (ptag(tp) == T_VAR) {
-        if (cas(tw, tp, bp) == tp) {
+    if (ptag(tp) == T_VAR) {
+      if (hcas(c, tw, tp, bp) == tp) {
+        tw = paddr(tp);
+        tp = hload(c, tw);
+        unsigned it2 = 0;
+        while (tp != P_LOCK && ptag(tp) == T_RED) {
+          half_free(c, tw);
           tw = paddr(tp);
-          tp = load(tw);
-          unsigned it2 = 0;
-          while (tp != P_LOCK && ptag(tp) == T_RED) {
-            half_free(tw);
-            tw = paddr(tp);
-            tp = load(tw);
-            if (!spin(it2)) return;
-          }
-          return;
-        }
-        if (!spin(it)) return;
-        continue;
-      }
-      if (principal(tp) || tp == P_GONE) {
-        ull xw = aw < tw ? aw : tw;
-        ull yw = aw < tw ? tw : aw;
-        ull xp = swap(xw, P_GONE);
-        if (xp != P_GONE) {
-          ull yp = swap(yw, P_GONE);
-          redux(xp, yp);
-        } else {
-          half_free(xw);
-          unsigned it3 = 0;
-          while (cas(yw, P_GONE, P_LOCK) != P_GONE)
-            if (!spin(it3)) return;
-          half_free(yw);
+          tp = hload(c, tw);
+          if (!run_spin(c.net, it2)) return;
         }
         return;
       }
-      fail(HVM64_ERR_BAD_PAIR, tp);
-      return;
+      if (!run_spin(c.net, it)) return;
+      continue;
     }
-  }
-  HVM_DEV void link_trg_port(ull a, ull b) {
-    if (trg_is_wire(a)) link_wire_port(a, b);
-    else link_port_port(a, b);
-  }
-  HVM_DEV void link_trg(ull a, ull b) {
-    bool aw = trg_is_wire(a), bw = trg_is_wire(b);
-    if (aw && bw) link_wire_wire(a, b);
-    else if (aw) link_wire_port(a, b);
-    else if (bw) link_wire_port(b, a);
-    else link_port_port(a, b);
-  }
-  HVM_DEV ull trg_target(ull t) { return trg_is_wire(t) ? load(t) : t; }
-  // The target of a Trg about to be consumed by a VM instruction.  A wire is
-  // locked rather than read: every path of the instruction then either frees
-  // that wire or links it at once (which would lock it first), so taking the
-  // lock up front saves a round trip and changes nothing observable.
-  HVM_DEV ull trg_take(ull t) { return trg_is_wire(t) ? lock_target(t) : t; }
-  // link_trg_port for a Trg taken with trg_take (its target already known).
-  HVM_DEV void link_taken(ull t, ull target, ull b) {
-    if (!trg_is_wire(t)) return link_port_port(t, b);
-    if (principal(target) && principal(b)) {
-      half_free(t);
-      redux(target, b);
-    } else {
-      half_link_wire_port(target, t, b);
-      half_link_port_port(b, target);
-    }
-  }
-  HVM_DEV void free_trg(ull t) {
-    if (trg_is_wire(t)) half_free(t);
-  }
-
-  // ---- rules (runtime/src/interact.rs) ----------------------------------------
-  HVM_DEV void anni2(ull a, ull b) {  // interact.rs:72-79
-    count(&W->rw[RW_ANNI], 1);
-    ull a1 = paddr(a), b1 = paddr(b);
-    link_wire_wire(a1, b1);
-    link_wire_wire(a1 ^ 8, b1 ^ 8);
-  }
-  HVM_DEV void comm22(ull a, ull b) {  // interact.rs:118-141
-    count(&W->rw[RW_COMM], 1);
-    count(&W->rw[EX_COMM22], 1);
-    ull a1 = paddr(a), b1 = paddr(b);
-    ull A1 = alloc(), A2 = alloc(), B1 = alloc(), B2 = alloc();
-    unsigned ta = ptag(a), la = plab(a), tb = ptag(b), lb = plab(b);
-    link_port_port(pvar(A1), pvar(B1));
-    link_port_port(pvar(A1 ^ 8), pvar(B2));
-    link_port_port(pvar(A2), pvar(B1 ^ 8));
-    link_port_port(pvar(A2 ^ 8), pvar(B2 ^ 8));
-    link_wire_port(a1, mkport(tb, lb, B1));
-    link_wire_port(a1 ^ 8, mkport(tb, lb, B2));
-    link_wire_port(b1, mkport(ta, la, A1));
-    link_wire_port(b1 ^ 8, mkport(ta, la, A2));
-  }
-  HVM_DEV void comm02(ull a, ull b) {  // interact.rs:162-168
-    count(&W->rw[RW_COMM], 1);
-    ull b1 = paddr(b);
-    link_wire_port(b1, a);
-    link_wire_port(b1 ^ 8, a);
-  }
-  HVM_DEV void switch_num(ull a, ull b) {  // interact.rs:201-223
-    count(&W->rw[RW_OPER], 1);
-    ull a1 = paddr(a);
-    uint32_t num = uint32_t(b);
-    uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
-    if (n == 0) {
-      ull x = alloc();
-      link_port_port(pvar(x ^ 8), P_ERA);
-      link_wire_port(a1 ^ 8, pvar(x));
-      link_wire_port(a1, mkport(T_CTR, 0, x));
-    } else {
-      ull x = alloc(), y = alloc();
-      link_port_port(pvar(x), P_ERA);
-      link_port_port(pvar(x ^ 8), mkport(T_CTR, 0, y));
-      link_port_port(pvar(y), ull(num_u24(n - 1)));
-      link_wire_port(a1 ^ 8, pvar(y ^ 8));
-      link_wire_port(a1, mkport(T_CTR, 0, x));
-    }
-  }
-  HVM_DEV uint32_t binary(uint32_t a, uint32_t op, uint32_t b) {
-    int e = 0;
-    uint32_t r = num_binary(a, op, b, &e);
-    if (e) fail(HVM64_ERR_DIV0, net);
-    return r;
-  }
-  HVM_DEV void op_num(ull a, ull b) {  // interact.rs:251-270
-    uint32_t op = plab(a);
-    ull a1 = paddr(a);
-    ull t1 = load(a1);
-    if (ptag(t1) == T_NUM) {
-      count(&W->rw[RW_OPER], 1);
-      half_free(a1);
-      ull out = binary(uint32_t(b), op, uint32_t(t1));
-      link_wire_port(a1 ^ 8, out);
-    } else {
-      ull x = alloc();
-      link_port_port(pvar(x), ull(num_unary(op, uint32_t(b))));
-      link_wire_port(a1 ^ 8, pvar(x ^ 8));
-      link_wire_port(a1, mkport(T_OP, NT_SYM, x));
-    }
-  }
-
-  // def.rs:30-37 (LabSet::has); the expansion agent's set is LabSet::ALL.
-  HVM_DEV bool def_has(ull ref, unsigned lab) {
-    if (ref & X_BIT) return lab < 0xFFFF;
-    unsigned id = unsigned((paddr(ref) >> 3) - 1);
-    if (id >= P.ndefs) {
-      fail(HVM64_ERR_BAD_INPUT, ref);
-      return true;
-    }
-    const DevDef& d = P.defs[id];
-    if (lab >= d.min_safe) return false;
-    unsigned w = lab >> 6;
-    if (w >= d.lab_len) return false;
-    return (P.labbits[d.lab_off + w] >> (lab & 63)) & 1;
-  }
-  // def.rs:177-189
-  HVM_DEV void call(ull port, ull trg) {
-    if (ptag(trg) == T_CTR && !def_has(port, plab(trg))) return comm02(port, trg);
-    count(&W->rw[RW_DREF], 1);
-    if (port & X_BIT) return expand_call(port, trg);
-    unsigned before = allocs;
-    run_def(unsigned((paddr(port) >> 3) - 1), trg);
-    count(&W->rw[EX_DNODES], allocs - before);
-  }
-
-  // ---- interact.rs:6-44 --------------------------------------------------------
-  HVM_DEV void interact(ull a, ull b) {
-    unsigned at = ptag(a), bt = ptag(b);
-    if (at <= T_VAR || bt <= T_VAR) return fail(HVM64_ERR_BAD_PAIR, a);
-    bool an = at == T_REF || at == T_NUM, bn = bt == T_REF || bt == T_NUM;
-    if (at == T_REF && bn && !skippable(a)) return call(a, b);
-    if (an && bt == T_REF && !skippable(b)) return call(b, a);
-    if (an && bn) {
-      count(&W->rw[RW_ERAS], 1);
-      return;
-    }
-    if (at == T_CTR && bt == T_SWITCH && plab(a) != 0) return comm22(a, b);
-    if (at == T_SWITCH && bt == T_CTR && plab(b) != 0) return comm22(a, b);
-    if ((at == T_CTR && bt == T_OP) || (at == T_OP && bt == T_CTR)) return comm22(a, b);
-    if (at == T_CTR && bt == T_CTR && plab(a) != plab(b)) return comm22(a, b);
-    if (at == bt && at >= T_OP) return anni2(a, b);
-    if (at == T_REF && bt == T_CTR && plab(b) >= plab(a)) return comm02(a, b);
-    if (at == T_CTR && bt == T_REF && plab(a) >= plab(b)) return comm02(b, a);
-    if (at == T_NUM && bt == T_CTR) return comm02(a, b);
-    if (at == T_CTR && bt == T_NUM) return comm02(b, a);
-    if (at == T_REF && a == P_ERA) return comm02(a, b);
-    if (bt == T_REF && b == P_ERA) return comm02(b, a);
-    if (at == T_REF) return call(a, b);
-    if (bt == T_REF) return call(b, a);
-    if (at == T_OP && bt == T_NUM) return op_num(a, b);
-    if (at == T_NUM && bt == T_OP) return op_num(b, a);
-    if (at == T_SWITCH && bt == T_NUM) return switch_num(a, b);
-    if (at == T_NUM && bt == T_SWITCH) return switch_num(b, a);
-    fail(HVM64_ERR_BAD_PAIR, a);
-  }
-
-  // ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) ----
-  HVM_DEV void do_ctr(unsigned lab, ull trg, ull& o1, ull& o2) {
-    ull port = trg_take(trg);
-    if (ptag(port) == T_CTR && plab(port) == lab) {
-      free_trg(trg);
-      count(&W->rw[RW_ANNI], 1);
-      o1 = paddr(port);  // Trg::wire
-      o2 = paddr(port) ^ 8;
-      return;
-    }
-    ull n = alloc();
-    link_taken(trg, port, mkport(T_CTR, lab, n));
-    o1 = pvar(n);
-    o2 = pvar(n ^ 8);
-  }
-  HVM_DEV void do_op(unsigned op, ull trg, ull& o1, ull& o2) {
-    ull port = trg_take(trg);
-    if (ptag(port) == T_NUM) {
-      free_trg(trg);
-      ull n = alloc();
-      store(n, ull(num_unary(op, uint32_t(port))));
-      o1 = mkport(T_OP, NT_SYM, n);
-      o2 = pvar(n ^ 8);
-      return;
-    }
-    if (port == P_ERA) {
-      free_trg(trg);
-      o1 = o2 = P_ERA;
-      return;
-    }
-    ull n = alloc();
-    link_taken(trg, port, mkport(T_OP, op, n));
-    o1 = pvar(n);
-    o2 = pvar(n ^ 8);
-  }
-  HVM_DEV ull do_op_num(unsigned op, ull trg, uint32_t rhs) {
-    ull port = trg_take(trg);
-    if (ptag(port) == T_NUM) {
-      count(&W->rw[RW_OPER], 1);
-      free_trg(trg);
-      return ull(binary(uint32_t(port), op, rhs));
-    }
-    if (port == P_ERA) {
-      free_trg(trg);
-      return P_ERA;
-    }
-    ull n = alloc();
-    link_taken(trg, port, mkport(T_OP, op, n));
-    store(n, ull(rhs));
-    return pvar(n ^ 8);
-  }
-  HVM_DEV ull create_wire_to(ull port) {  // node.rs:176-182
-    ull a = alloc();
-    half_free(a ^ 8);
-    link_port_port(port, pvar(a));
-    return a;
-  }
-  HVM_DEV void do_switch(ull trg, ull& o1, ull& o2) {
-    ull port = trg_take(trg);
-    if (ptag(port) == T_NUM) {
-      count(&W->rw[RW_OPER], 1);
-      free_trg(trg);
-      uint32_t num = uint32_t(port);
-      uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
-      ull c1 = alloc();
-      if (n == 0) {
-        link_port_port(pvar(c1 ^ 8), P_ERA);
-        o1 = mkport(T_CTR, 0, c1);
-        o2 = create_wire_to(pvar(c1));
+    if (principal(tp) || tp == P_GONE) {
+      ull xw = aw < tw ? aw : tw;
+      ull yw = aw < tw ? tw : aw;
+      ull xp = hswap(c, xw, P_GONE);
+      if (xp != P_GONE) {
+        ull yp = hswap(c, yw, P_GONE);
+        redux(c, xp, yp);
       } else {
-        ull c2 = alloc();
-        link_port_port(pvar(c1), P_ERA);
-        link_port_port(pvar(c1 ^ 8), mkport(T_CTR, 0, c2));
-        link_port_port(pvar(c2), ull(num_u24(n - 1)));
-        o1 = mkport(T_CTR, 0, c1);
-        o2 = create_wire_to(pvar(c2 ^ 8));
+        half_free(c, xw);
+        unsigned it3 = 0;
+        while (hcas(c, yw, P_GONE, P_LOCK) != P_GONE)
+          if (!run_spin(c.net, it3)) return;
+        half_free(c, yw);
       }
       return;
     }
-    if (port == P_ERA) {
-      count(&W->rw[RW_ERAS], 1);
-      free_trg(trg);
-      o1 = o2 = P_ERA;
-      return;
-    }
-    ull m = alloc();
-    link_taken(trg, port, mkport(T_SWITCH, 0, m));
-    o1 = pvar(m);
-    o2 = pvar(m ^ 8);
+    run_fail(c.net, HVM64_ERR_BAD_PAIR, tp);
+    return;
   }
+}
+// Trg (linker.rs:228-304): a wire is its address with the Red tag.
+HVM_INL void link_trg_port(const Ctx& c, ull a, ull b) {
+  if (trg_is_wire(a)) link_wire_port(c, a, b);
+  else link_port_port(c, a, b);
+}
+HVM_COLD void link_trg(const Ctx& c, ull a, ull b) {
+  bool aw = trg_is_wire(a), bw = trg_is_wire(b);
+  if (aw && bw) link_wire_wire(c, a, b);
+  else if (aw) link_wire_port(c, a, b);
+  else if (bw) link_wire_port(c, b, a);
+  else link_port_port(c, a, b);
+}
+HVM_INL void free_trg(const Ctx& c, ull t) {
+  if (trg_is_wire(t)) half_free(c, t);
+}
+// The target of a Trg about to be consumed by a VM instruction.  A wire is
+// locked rather than read: every path of the instruction then either frees
+// that wire or links it at once (which would lock it first), so taking the
+// lock up front saves a round trip and changes nothing observable.
+HVM_INL ull trg_take(const Ctx& c, ull t) { return trg_is_wire(t) ? lock_target(c, t) : t; }
+// link_trg_port for a Trg taken with trg_take.
+HVM_INL void link_taken(const Ctx& c, ull t, ull target, ull b) {
+  if (trg_is_wire(t)) link_locked_wire_port(c, t, target, b);
+  else link_port_port(c, t, b);
+}
 
-  HVM_DEV void run_def(unsigned id, ull t0) {
-    if (id >= P.ndefs) return fail(HVM64_ERR_BAD_INPUT, id);
-    const DevDef d = P.defs[id];
-    if (d.nregs <= SMALL_REGS) {
-      exec(d, t0, StridedRegs{W->regs + lane, 32});
+// ---- rules (runtime/src/interact.rs) ------------------------------------------
+HVM_COLD void anni2(const Ctx& c, ull a, ull b) {  // interact.rs:72-79
+  count(c, RW_ANNI);
+  ull a1 = paddr(a), b1 = paddr(b);
+  link_wire_wire(c, a1, b1);
+  link_wire_wire(c, a1 ^ 8, b1 ^ 8);
+}
+HVM_COLD void comm22(const Ctx& c, ull a, ull b) {  // interact.rs:118-141
+  count(c, RW_COMM);
+  count(c, EX_COMM22);
+  ull a1 = paddr(a), b1 = paddr(b);
+  ull A1 = alloc(c), A2 = alloc(c), B1 = alloc(c), B2 = alloc(c);
+  unsigned ta = ptag(a), la = plab(a), tb = ptag(b), lb = plab(b);
+  link_port_port(c, pvar(A1), pvar(B1));
+  link_port_port(c, pvar(A1 ^ 8), pvar(B2));
+  link_port_port(c, pvar(A2), pvar(B1 ^ 8));
+  link_port_port(c, pvar(A2 ^ 8), pvar(B2 ^ 8));
+  link_wire_port(c, a1, mkport(tb, lb, B1));
+  link_wire_port(c, a1 ^ 8, mkport(tb, lb, B2));
+  link_wire_port(c, b1, mkport(ta, la, A1));
+  link_wire_port(c, b1 ^ 8, mkport(ta, la, A2));
+}
+HVM_COLD void comm02(const Ctx& c, ull a, ull b) {  // interact.rs:162-168
+  count(c, RW_COMM);
+  ull b1 = paddr(b);
+  link_wire_port(c, b1, a);
+  link_wire_port(c, b1 ^ 8, a);
+}
+HVM_COLD void switch_num(const Ctx& c, ull a, ull b) {  // interact.rs:201-223
+  count(c, RW_OPER);
+  ull a1 = paddr(a);
+  uint32_t num = uint32_t(b);
+  uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
+  if (n == 0) {
+    ull x = alloc(c);
+    link_port_port(c, pvar(x ^ 8), P_ERA);
+    link_wire_port(c, a1 ^ 8, pvar(x));
+    link_wire_port(c, a1, mkport(T_CTR, 0, x));
+  } else {
+    ull x = alloc(c), y = alloc(c);
+    link_port_port(c, pvar(x), P_ERA);
+    link_port_port(c, pvar(x ^ 8), mkport(T_CTR, 0, y));
+    link_port_port(c, pvar(y), ull(num_u24(n - 1)));
+    link_wire_port(c, a1 ^ 8, pvar(y ^ 8));
+    link_wire_port(c, a1, mkport(T_CTR, 0, x));
+  }
+}
+HVM_COLD void op_num(const Ctx& c, ull a, ull b) {  // interact.rs:251-270
+  uint32_t op = plab(a);
+  ull a1 = paddr(a);
+  ull t1 = hload(c, a1);
+  if (ptag(t1) == T_NUM) {
+    count(c, RW_OPER);
+    half_free(c, a1);
+    ull out = binary_op(c.net, uint32_t(b), op, uint32_t(t1));
+    link_wire_port(c, a1 ^ 8, out);
+  } else {
+    ull x = alloc(c);
+    link_port_port(c, pvar(x), ull(num_unary(op, uint32_t(b))));
+    link_wire_port(c, a1 ^ 8, pvar(x ^ 8));
+    link_wire_port(c, a1, mkport(T_OP, NT_SYM, x));
+  }
+}
+
+// ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) -----
+HVM_COLD void do_ctr(const Ctx& c, unsigned lab, ull trg, ull& o1, ull& o2) {
+  ull port = trg_take(c, trg);
+  if (ptag(port) == T_CTR && plab(port) == lab) {
+    free_trg(c, trg);
+    count(c, RW_ANNI);
+    o1 = paddr(port);  // Trg::wire
+    o2 = paddr(port) ^ 8;
+    return;
+  }
+  ull n = alloc(c);
+  link_taken(c, trg, port, mkport(T_CTR, lab, n));
+  o1 = pvar(n);
+  o2 = pvar(n ^ 8);
+}
+HVM_COLD void do_op(const Ctx& c, unsigned op, ull trg, ull& o1, ull& o2) {
+  ull port = trg_take(c, trg);
+  if (ptag(port) == T_NUM) {
+    free_trg(c, trg);
+    ull n = alloc(c);
+    hstore(c, n, ull(num_unary(op, uint32_t(port))));
+    o1 = mkport(T_OP, NT_SYM, n);
+    o2 = pvar(n ^ 8);
+    return;
+  }
+  if (port == P_ERA) {
+    free_trg(c, trg);
+    o1 = o2 = P_ERA;
+    return;
+  }
+  ull n = alloc(c);
+  link_taken(c, trg, port, mkport(T_OP, op, n));
+  o1 = pvar(n);
+  o2 = pvar(n ^ 8);
+}
+HVM_COLD ull do_op_num(const Ctx& c, unsigned op, ull trg, uint32_t rhs) {
+  ull port = trg_take(c, trg);
+  if (ptag(port) == T_NUM) {
+    count(c, RW_OPER);
+    free_trg(c, trg);
+    return ull(binary_op(c.net, uint32_t(port), op, rhs));
+  }
+  if (port == P_ERA) {
+    free_trg(c, trg);
+    return P_ERA;
+  }
+  ull n = alloc(c);
+  link_taken(c, trg, port, mkport(T_OP, op, n));
+  hstore(c, n, ull(rhs));
+  return pvar(n ^ 8);
+}
+HVM_COLD ull create_wire_to(const Ctx& c, ull port) {  // node.rs:176-182
+  ull a = alloc(c);
+  half_free(c, a ^ 8);
+  link_port_port(c, port, pvar(a));
+  return a;
+}
+HVM_COLD void do_switch(const Ctx& c, ull trg, ull& o1, ull& o2) {
+  ull port = trg_take(c, trg);
+  if (ptag(port) == T_NUM) {
+    count(c, RW_OPER);
+    free_trg(c, trg);
+    uint32_t num = uint32_t(port);
+    uint32_t n = num_tag(num) == NT_U24 ? num_payload(num) : 0;
+    ull c1 = alloc(c);
+    if (n == 0) {
+      link_port_port(c, pvar(c1 ^ 8), P_ERA);
+      o1 = mkport(T_CTR, 0, c1);
+      o2 = create_wire_to(c, pvar(c1));
     } else {
-      ull R[MAX_REGS];
-      exec(d, t0, StridedRegs{R, 1});
+      ull c2 = alloc(c);
+      link_port_port(c, pvar(c1), P_ERA);
+      link_port_port(c, pvar(c1 ^ 8), mkport(T_CTR, 0, c2));
+      link_port_port(c, pvar(c2), ull(num_u24(n - 1)));
+      o1 = mkport(T_CTR, 0, c1);
+      o2 = create_wire_to(c, pvar(c2 ^ 8));
     }
+    return;
   }
-  HVM_DEV void exec(const DevDef& d, ull t0, StridedRegs R) {
-    R[0] = t0;
-    const DevInstr* ins = P.instrs + d.ins_off;
-    for (unsigned k = 0; k < d.ins_len; k++) {
-      const DevInstr I = ins[k];
-      switch (I.k) {
-        case I_CONST: R[I.a] = I.port; break;
-        case I_LINK: count(&W->rw[EX_DLINKS], 1); link_trg(R[I.a], R[I.b]); break;
-        case I_LINKCONST: count(&W->rw[EX_DLINKS], 1); link_trg_port(R[I.a], I.port); break;
-        case I_CTR: {
-          ull x, y;
-          do_ctr(I.lab, R[I.a], x, y);
-          R[I.b] = x;
-          R[I.c] = y;
-          break;
-        }
-        case I_OP: {
-          ull x, y;
-          do_op(I.op, R[I.a], x, y);
-          R[I.b] = x;
-          R[I.c] = y;
-          break;
-        }
-        case I_OPNUM: R[I.c] = do_op_num(I.op, R[I.a], uint32_t(I.port)); break;
-        case I_SWITCH: {
-          ull x, y;
-          do_switch(R[I.a], x, y);
-          R[I.b] = x;
-          R[I.c] = y;
-          break;
-        }
-        case I_WIRES: {
-          ull a = alloc();
-          R[I.a] = pvar(a);
-          R[I.b] = a;
-          R[I.c] = pvar(a ^ 8);
-          R[I.d] = a ^ 8;
-          break;
-        }
+  if (port == P_ERA) {
+    count(c, RW_ERAS);
+    free_trg(c, trg);
+    o1 = o2 = P_ERA;
+    return;
+  }
+  ull m = alloc(c);
+  link_taken(c, trg, port, mkport(T_SWITCH, 0, m));
+  o1 = pvar(m);
+  o2 = pvar(m ^ 8);
+}
+// Runs a Def's instruction list over a register file (base + i * stride).
+HVM_COLD void exec(const Ctx& c, const DevDef& d, ull t0, ull* R, unsigned stride, const DevInstr* ins) {
+  R[0] = t0;
+  for (unsigned k = 0; k < d.ins_len; k++) {
+    const DevInstr I = ins[k];
+    ull* ra = R + I.a * stride;
+    switch (I.k) {
+      case I_CONST: *ra = I.port; break;
+      case I_LINK: count(c, EX_DLINKS); link_trg(c, *ra, R[I.b * stride]); break;
+      case I_LINKCONST: count(c, EX_DLINKS); link_trg_port(c, *ra, I.port); break;
+      case I_CTR: do_ctr(c, I.lab, *ra, R[I.b * stride], R[I.c * stride]); break;
+      case I_OP: do_op(c, I.op, *ra, R[I.b * stride], R[I.c * stride]); break;
+      case I_OPNUM: R[I.c * stride] = do_op_num(c, I.op, *ra, uint32_t(I.port)); break;
+      case I_SWITCH: do_switch(c, *ra, R[I.b * stride], R[I.c * stride]); break;
+      case I_WIRES: {
+        ull a = alloc(c);
+        R[I.a * stride] = pvar(a);
+        R[I.b * stride] = a;
+        R[I.c * stride] = pvar(a ^ 8);
+        R[I.d * stride] = a ^ 8;
+        break;
       }
     }
   }
+}
+HVM_COLD void exec_large(const Ctx& c, const DevDef& d, ull t0) {
+  ull R[MAX_REGS];
+  exec(c, d, t0, R, 1, g_P.instrs + d.ins_off);
+}
+HVM_COLD void run_def(const Ctx& c, unsigned id, ull t0) {
+  if (id >= g_P.ndefs) return run_fail(c.net, HVM64_ERR_BAD_INPUT, id);
+  ull* R = c.W->regs + c.lane;
+  if (id == c.W->icache_def) {  // staged by the warp for this step
+    const DevDef& d = c.W->idef;
+    if (d.nregs <= SMALL_REGS) return exec(c, d, t0, R, 32, c.W->icache);
+    return exec_large(c, d, t0);
+  }
+  const DevDef d = g_P.defs[id];
+  if (d.nregs <= SMALL_REGS) exec(c, d, t0, R, 32, g_P.instrs + d.ins_off);
+  else exec_large(c, d, t0);
+}
 
-  // ---- expansion agent (runtime/src/net.rs:63-108) ----------------------------
-  // An agent is a Ref port with X_BIT whose address names a heap word holding
-  // its output port (the reference boxes an `ExpandDef { out }`).
-  HVM_DEV ull new_expand(ull out) {
-    ull w = alloc();
-    half_free(w ^ 8);
-    store(w, out);
-    return mkport(T_REF, 0xFFFF, X_BIT | w);
+// def.rs:30-37 (LabSet::has); the expansion agent's set is LabSet::ALL.
+HVM_INL bool def_has(const Ctx& c, ull ref, unsigned lab) {
+  if (ref & X_BIT) return lab < 0xFFFF;
+  unsigned id = unsigned((paddr(ref) >> 3) - 1);
+  if (id >= g_P.ndefs) {
+    run_fail(c.net, HVM64_ERR_BAD_INPUT, ref);
+    return true;
   }
-  HVM_DEV ull take_expand(ull port) {
-    ull w = paddr(port) & ~X_BIT;
-    unsigned it = 0;
-    ull out;
-    while ((out = load(w)) == P_LOCK)
-      if (!spin(it)) break;
-    half_free(w);
-    return out;
-  }
-  HVM_DEV void expand_call(ull self, ull port) {
-    if (ptag(port) == T_REF && port != P_ERA) {
-      if (port & X_BIT) {
-        ull a = take_expand(self), b = take_expand(port);
-        return link_port_port(a, b);
-      }
-      return call(port, self);
+  const DevDef& d = g_P.defs[id];
+  if (lab >= d.min_safe) return false;
+  unsigned w = lab >> 6;
+  if (w >= d.lab_len) return false;
+  return (g_P.labbits[d.lab_off + w] >> (lab & 63)) & 1;
+}
+
+// ---- expansion agent (runtime/src/net.rs:63-108) ----------------------------
+// An agent is a Ref port with X_BIT whose address names a heap word holding
+// its output port (the reference boxes an `ExpandDef { out }`).
+HVM_COLD ull new_expand(const Ctx& c, ull out) {
+  ull w = alloc(c);
+  half_free(c, w ^ 8);
+  hstore(c, w, out);
+  return mkport(T_REF, 0xFFFF, X_BIT | w);
+}
+HVM_COLD ull take_expand(const Ctx& c, ull port) {
+  ull w = paddr(port) & ~X_BIT;
+  unsigned it = 0;
+  ull out;
+  while ((out = hload(c, w)) == P_LOCK)
+    if (!run_spin(c.net, it)) break;
+  half_free(c, w);
+  return out;
+}
+HVM_COLD void call(const Ctx& c, ull port, ull trg);
+HVM_COLD void expand_call(const Ctx& c, ull self, ull port) {
+  if (ptag(port) == T_REF && port != P_ERA) {
+    if (port & X_BIT) {
+      ull a = take_expand(c, self), b = take_expand(c, port);
+      return link_port_port(c, a, b);
     }
-    ull out = take_expand(self);
-    unsigned t = ptag(port);
-    if (t == T_RED) return fail(HVM64_ERR_BAD_PAIR, port);
-    if (t == T_REF || t == T_NUM || t == T_VAR) return link_port_port(out, port);
-    ull o1 = paddr(port);
-    ull n = alloc();
-    link_port_port(out, mkport(t, plab(port), n));
-    link_wire_port(o1, new_expand(pvar(n)));
-    link_wire_port(o1 ^ 8, new_expand(pvar(n ^ 8)));
+    return call(c, port, self);
   }
-  // net.rs:65-69
-  HVM_DEV ull expand(ull root) {
-    ull a = alloc();
-    half_free(a ^ 8);
-    link_wire_port(root, new_expand(pvar(a)));
-    return a;
-  }
-};
+  ull out = take_expand(c, self);
+  unsigned t = ptag(port);
+  if (t == T_RED) return run_fail(c.net, HVM64_ERR_BAD_PAIR, port);
+  if (t == T_REF || t == T_NUM || t == T_VAR) return link_port_port(c, out, port);
+  ull o1 = paddr(port);
+  ull n = alloc(c);
+  link_port_port(c, out, mkport(t, plab(port), n));
+  link_wire_port(c, o1, new_expand(c, pvar(n)));
+  link_wire_port(c, o1 ^ 8, new_expand(c, pvar(n ^ 8)));
+}
+// net.rs:65-69
+HVM_COLD ull expand(const Ctx& c, ull root) {
+  ull a = alloc(c);
+  half_free(c, a ^ 8);
+  link_wire_port(c, root, new_expand(c, pvar(a)));
+  return a;
+}
+// def.rs:177-189
+HVM_COLD void call(const Ctx& c, ull port, ull trg) {
+  if (ptag(trg) == T_CTR && !def_has(c, port, plab(trg))) return comm02(c, port, trg);
+  count(c, RW_DREF);
+  if (port & X_BIT) return expand_call(c, port, trg);
+  unsigned before = LS(allocs);
+  run_def(c, unsigned((paddr(port) >> 3) - 1), trg);
+  count(c, EX_DNODES, LS(allocs) - before);
+}
+
+// ---- interact.rs:6-44 ----------------------------------------------------------
+HVM_COLD void interact(const Ctx& c, ull a, ull b) {
+  unsigned at = ptag(a), bt = ptag(b);
+  if (at <= T_VAR || bt <= T_VAR) return run_fail(c.net, HVM64_ERR_BAD_PAIR, a);
+  bool an = at == T_REF || at == T_NUM, bn = bt == T_REF || bt == T_NUM;
+  if (at == T_REF && bn && !skippable(a)) return call(c, a, b);
+  if (an && bt == T_REF && !skippable(b)) return call(c, b, a);
+  if (an && bn) return count(c, RW_ERAS);
+  if (at == T_CTR && bt == T_SWITCH && plab(a) != 0) return comm22(c, a, b);
+  if (at == T_SWITCH && bt == T_CTR && plab(b) != 0) return comm22(c, a, b);
+  if ((at == T_CTR && bt == T_OP) || (at == T_OP && bt == T_CTR)) return comm22(c, a, b);
+  if (at == T_CTR && bt == T_CTR && plab(a) != plab(b)) return comm22(c, a, b);
+  if (at == bt && at >= T_OP) return anni2(c, a, b);
+  if (at == T_REF && bt == T_CTR && plab(b) >= plab(a)) return comm02(c, a, b);
+  if (at == T_CTR && bt == T_REF && plab(a) >= plab(b)) return comm02(c, b, a);
+  if (at == T_NUM && bt == T_CTR) return comm02(c, a, b);
+  if (at == T_CTR && bt == T_NUM) return comm02(c, b, a);
+  if (at == T_REF && a == P_ERA) return comm02(c, a, b);
+  if (bt == T_REF && b == P_ERA) return comm02(c, b, a);
+  if (at == T_REF) return call(c, a, b);
+  if (bt == T_REF) return call(c, b, a);
+  if (at == T_OP && bt == T_NUM) return op_num(c, a, b);
+  if (at == T_NUM && bt == T_OP) return op_num(c, b, a);
+  if (at == T_SWITCH && bt == T_NUM) return switch_num(c, a, b);
+  if (at == T_NUM && bt == T_SWITCH) return switch_num(c, b, a);
+  run_fail(c.net, HVM64_ERR_BAD_PAIR, a);
+}
+
+#undef LS
+#undef FW
 
 }  // namespace dev
 }  // namespace hvm

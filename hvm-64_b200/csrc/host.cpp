@@ -609,7 +609,7 @@ static void emit(Book& book, const std::vector<RawInstr>& raw, uint32_t nregs, D
     x.k = r.k;
     x.op = r.op;
     x.lab = r.lab;
-    x.a = r.a; x.b = r.b; x.c = r.c; x.d = r.d;
+    x.a = uint8_t(r.a); x.b = uint8_t(r.b); x.c = uint8_t(r.c); x.d = uint8_t(r.d);
     x.port = r.port;
     book.instrs.push_back(x);
     nodes += r.k == I_SWITCH ? 3 : (r.k == I_CTR || r.k == I_OP || r.k == I_OPNUM || r.k == I_WIRES) ? 1 : 0;

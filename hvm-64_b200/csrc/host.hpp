@@ -39,12 +39,11 @@ inline uint64_t ref_port(uint32_t def_id, uint16_t min_safe) { return port_new(T
 // once), register 0 being the Def's argument port.
 enum InstrKind : uint8_t { I_CONST, I_LINK, I_LINKCONST, I_CTR, I_OP, I_OPNUM, I_SWITCH, I_WIRES };
 
-struct DevInstr {  // 32 bytes
+struct DevInstr {  // 16 bytes
   uint8_t k;
   uint8_t op;    // NumTag for Op / OpNum
   uint16_t lab;  // Ctr label
-  uint32_t a, b, c, d;
-  uint32_t pad;
+  uint8_t a, b, c, d;  // registers
   uint64_t port;  // Const / LinkConst port, OpNum right operand (low 32 bits)
 };
 
@@ -57,7 +56,7 @@ struct DevDef {  // 32 bytes
   uint32_t nodes;  // upper bound on nodes one call allocates
   uint32_t redexes;
 };
-static_assert(sizeof(DevInstr) == 32, "DevInstr layout");
+static_assert(sizeof(DevInstr) == 16, "DevInstr layout");
 static_assert(sizeof(DevDef) == 32, "DevDef layout");
 
 constexpr uint32_t MAX_REGS = 48;  // device register file per call

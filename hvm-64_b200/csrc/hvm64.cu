@@ -32,13 +32,13 @@ namespace dev {
 
 // ---- global redex queue --------------------------------------------------------
 // Single-thread reservation; data movement may be done by the whole warp.
-__device__ bool q_reserve_push(const Params& P, Lane& L, ull& pos, bool must) {
-  Ctrl* C = P.ctrl;
+__device__ bool q_reserve_push(unsigned net, ull& pos, bool must) {
+  Ctrl* C = g_P.ctrl;
   ull mask = C->q_mask;
   pos = ld_gpu(&C->q_tail);
   unsigned it = 0;
   for (;;) {
-    Slot* s = &P.q[pos & mask];
+    Slot* s = &g_P.q[pos & mask];
     long long dif = (long long)ld_gpu(&s->seq) - (long long)pos;
     if (dif == 0) {
       ull old = atomicCAS(&C->q_tail, pos, pos + 1);
@@ -50,22 +50,22 @@ __device__ bool q_reserve_push(const Params& P, Lane& L, ull& pos, bool must) {
     } else {
       pos = ld_gpu(&C->q_tail);
     }
-    if (!L.spin(it)) {
-      if (must && !L.failed()) L.fail(HVM64_ERR_QUEUE, pos);
+    if (!run_spin(net, it)) {
+      if (must && !run_failed()) run_fail(net, HVM64_ERR_QUEUE, pos);
       return false;
     }
   }
 }
-__device__ void q_publish(const Params& P, ull pos) {
+__device__ void q_publish(ull pos) {
   __threadfence();
-  st_gpu(&P.q[pos & P.ctrl->q_mask].seq, pos + 1);
+  st_gpu(&g_P.q[pos & g_P.ctrl->q_mask].seq, pos + 1);
 }
-__device__ bool q_reserve_pop(const Params& P, ull& pos) {
-  Ctrl* C = P.ctrl;
+__device__ bool q_reserve_pop(ull& pos) {
+  Ctrl* C = g_P.ctrl;
   ull mask = C->q_mask;
   pos = ld_gpu(&C->q_head);
   for (int tries = 0; tries < 64; tries++) {
-    Slot* s = &P.q[pos & mask];
+    Slot* s = &g_P.q[pos & mask];
     long long dif = (long long)ld_gpu(&s->seq) - (long long)(pos + 1);
     if (dif == 0) {
       ull old = atomicCAS(&C->q_head, pos, pos + 1);
@@ -79,42 +79,42 @@ __device__ bool q_reserve_pop(const Params& P, ull& pos) {
   }
   return false;
 }
-__device__ void q_release(const Params& P, ull pos) {
+__device__ void q_release(ull pos) {
   __threadfence();
-  st_gpu(&P.q[pos & P.ctrl->q_mask].seq, pos + P.ctrl->q_mask + 1);
+  st_gpu(&g_P.q[pos & g_P.ctrl->q_mask].seq, pos + g_P.ctrl->q_mask + 1);
 }
 
 // The warp's stack is full: ship one redex as its own slot (rare: each step
 // starts with HEADROOM free stack slots).
-__device__ void Lane::overflow_one(ull a, ull b) {
-  atomicAdd(reinterpret_cast<ull*>(&P.nets[net].pending), 1ull);
+__device__ __noinline__ void push_overflow(unsigned net, ull a, ull b) {
+  atomicAdd(reinterpret_cast<ull*>(&g_P.nets[net].pending), 1ull);
   ull pos;
-  if (!q_reserve_push(P, *this, pos, true)) return;
-  Slot* s = &P.q[pos & P.ctrl->q_mask];
+  if (!q_reserve_push(net, pos, true)) return;
+  Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
   st_gpu(reinterpret_cast<ull*>(&s->net), (1ull << 32) | net);
   st_gpu(&s->r[0], a);
   st_gpu(&s->r[1], b);
-  q_publish(P, pos);
-  atomicAdd(&P.ctrl->stat_overflow, 1ull);
+  q_publish(pos);
+  atomicAdd(&g_P.ctrl->stat_overflow, 1ull);
 }
 
 __device__ __forceinline__ ull shfl(ull v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 
 // Warp-cooperative: move the `cnt` oldest redexes of the warp's stack into a
 // queue slot.  Returns false if the queue had no room (only when !must).
-__device__ bool donate(const Params& P, Lane& L, ull* S, unsigned& bot, unsigned cnt, int cur, bool must) {
+__device__ bool donate(ull* S, unsigned& bot, unsigned cnt, int cur, bool must) {
   const unsigned lane = threadIdx.x & 31;
   ull pos = 0;
   int ok = 0;
   if (lane == 0) {
-    atomicAdd(reinterpret_cast<ull*>(&P.nets[cur].pending), 1ull);
-    ok = q_reserve_push(P, L, pos, must) ? 1 : 0;
-    if (!ok) atomicAdd(reinterpret_cast<ull*>(&P.nets[cur].pending), ~0ull);
+    atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), 1ull);
+    ok = q_reserve_push(unsigned(cur), pos, must) ? 1 : 0;
+    if (!ok) atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), ~0ull);
   }
   ok = __shfl_sync(0xffffffffu, ok, 0);
   if (!ok) return false;
   pos = shfl(pos, 0);
-  Slot* s = &P.q[pos & P.ctrl->q_mask];
+  Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
   if (lane < cnt) {
     unsigned k = (bot + lane) & (SCAP - 1);
     st_gpu(&s->r[2 * lane], S[2 * k]);
@@ -123,18 +123,18 @@ __device__ bool donate(const Params& P, Lane& L, ull* S, unsigned& bot, unsigned
   if (lane == 0) st_gpu(reinterpret_cast<ull*>(&s->net), (ull(cnt) << 32) | unsigned(cur));
   __threadfence();
   __syncwarp();
-  if (lane == 0) q_publish(P, pos);
+  if (lane == 0) q_publish(pos);
   bot += cnt;
   return true;
 }
 
 // Flush the warp's counters into its net (one atomic per counter).
-__device__ void flush_counters(const Params& P, WarpSmem& W, int cur) {
+__device__ void flush_counters(WarpSmem& W, int cur) {
   const unsigned lane = threadIdx.x & 31;
   __syncwarp();
   if (lane < unsigned(NCOUNT)) {
     ull v = W.rw[lane];
-    if (v) atomicAdd(&P.nets[cur].rw[lane], v);
+    if (v) atomicAdd(&g_P.nets[cur].rw[lane], v);
     W.rw[lane] = 0;
   }
   __syncwarp();
@@ -143,20 +143,28 @@ __device__ void flush_counters(const Params& P, WarpSmem& W, int cur) {
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 56 * 1024, "four reducer blocks per SM must fit in shared memory");
 
-__global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
+__global__ void __launch_bounds__(THREADS, 4) reduce_kernel() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u, gt = ~lt & ~(1u << lane);
   ull* S = W.stk;
-  Ctrl* C = P.ctrl;
-  Lane L(P, &W, lane);
+  Ctrl* C = g_P.ctrl;
+  Ctx c{&W, lane, 0};
+  lane_init(&W, lane);
   if (lane < unsigned(NCOUNT)) W.rw[lane] = 0;
+#ifdef HVM_PROFILE_OPS
+  if (lane < 8) W.prof[lane] = 0;
+#endif
   if (lane == 0) {
     W.pool_n = 0;
     W.freed_n = 0;
     W.ring_cnt = 0;
-    W.st_steps = W.st_lanes = W.st_busy = W.st_idle = 0;
+    W.icache_def = ~0u;
+    W.pool_cap = POOL;
+    W.ring_base = 0;
+    W.ring_cap = 0;
+    W.st_steps = W.st_lanes = W.st_busy = W.st_idle = W.st_lane_sum = W.st_lane_max = 0;
   }
   __syncwarp();
   unsigned top = 0, bot = 0;  // warp-uniform ring indices
@@ -165,6 +173,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
   unsigned idle = 0, step = 0;
   // Deadline from this launch's start (a replayed launch gets a fresh one).
   const ull deadline = globaltimer() + C->timeout_ns;
+  const long long born = clock64();
   unsigned nap = 0;  // idle backoff, ns
 
   for (;;) {
@@ -178,16 +187,16 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
 
     if (top == bot) {
       if (cur >= 0) {
-        flush_counters(P, W, cur);
+        flush_counters(W, cur);
         if (lane == 0) {
-          long long old = (long long)atomicAdd(reinterpret_cast<ull*>(&P.nets[cur].pending), ~0ull);
+          long long old = (long long)atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), ~0ull);
           if (old == 1) atomicAdd(reinterpret_cast<ull*>(&C->nets_left), ~0ull);
         }
         cur = -1;
       }
       ull pos = 0;
       int got = 0;
-      if (lane == 0) got = q_reserve_pop(P, pos) ? 1 : 0;
+      if (lane == 0) got = q_reserve_pop(pos) ? 1 : 0;
       got = __shfl_sync(0xffffffffu, got, 0);
       if (!got) {
         // Idle: back off exponentially (1 us .. 64 us) so that waiting warps
@@ -197,7 +206,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
           if (!hungry) atomicAdd(reinterpret_cast<ull*>(&C->hungry), 1ull);
           if (ld_gpu64s(&C->nets_left) <= 0) stop = 1;
           else if ((++idle & 15) == 0 && globaltimer() > deadline) {
-            L.fail(HVM64_ERR_TIMEOUT, 1);
+            run_fail(0, HVM64_ERR_TIMEOUT, 1);
             stop = 1;
           }
           if (ld_gpu32(&C->error)) stop = 1;
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
       idle = 0;
       pos = shfl(pos, 0);
       __threadfence();
-      Slot* s = &P.q[pos & C->q_mask];
+      Slot* s = &g_P.q[pos & C->q_mask];
       unsigned cnt = 0, net = 0;
       if (lane == 0) {
         ull meta = ld_gpu(reinterpret_cast<const ull*>(&s->net));
@@ -225,8 +234,8 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
       }
       cnt = __shfl_sync(0xffffffffu, cnt, 0);
       net = __shfl_sync(0xffffffffu, net, 0);
-      if (net >= P.nnets || cnt > unsigned(CHUNK)) {  // never expected; refuse to index with it
-        if (lane == 0) L.fail(HVM64_ERR_BAD_ADDR, (ull(cnt) << 32) | net);
+      if (net >= g_P.nnets || cnt > unsigned(CHUNK)) {  // never expected; refuse to index with it
+        if (lane == 0) run_fail(net, HVM64_ERR_BAD_ADDR, (ull(cnt) << 32) | net);
         break;
       }
       if (lane < cnt) {
@@ -234,11 +243,11 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
         S[2 * lane + 1] = ld_gpu(&s->r[2 * lane + 1]);
       }
       __syncwarp();
-      if (lane == 0) q_release(P, pos);
+      if (lane == 0) q_release(pos);
       bot = 0;
       top = cnt;
       cur = int(net);
-      L.net = net;
+      c.net = net;
       if (cnt == 0) continue;
     }
 
@@ -246,7 +255,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
     if ((++step & 1023) == 0) {
       int late = 0;
       if (lane == 0 && globaltimer() > deadline) {
-        L.fail(HVM64_ERR_TIMEOUT, 2);
+        run_fail(unsigned(cur), HVM64_ERR_TIMEOUT, 2);
         late = 1;
       }
       if (__shfl_sync(0xffffffffu, late, 0)) break;
@@ -254,7 +263,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
 
     // Keep HEADROOM slots free for this step's new redexes.
     while ((top - bot) > unsigned(SCAP - HEADROOM)) {
-      if (!donate(P, L, S, bot, 32u, cur, true)) break;
+      if (!donate(S, bot, 32u, cur, true)) break;
       if (lane == 0) atomicAdd(&C->stat_spilled, 1ull);
     }
 
@@ -310,27 +319,55 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
       S[2 * k + 1] = b0;
     }
     top = base + unsigned(__popc(um0)) + unsigned(__popc(um1));
-    if (lane == 0) W.ring_cnt = 0;
+    if (lane == 0) {
+      W.ring_cnt = 0;
+      W.ring_base = top;
+      W.ring_cap = unsigned(SCAP) - (top - bot);
+    }
+    // A step of Def calls: stage that Def's instructions in shared memory
+    // (one cooperative load instead of a dependent fetch per instruction).
+    if (key >= 64u && key - 64u < g_P.ndefs && key - 64u != W.icache_def) {
+      unsigned id = key - 64u;
+      const DevDef d = g_P.defs[id];
+      if (d.ins_len <= ICACHE) {
+        const uint4* src = reinterpret_cast<const uint4*>(g_P.instrs + d.ins_off);
+        uint4* dst = reinterpret_cast<uint4*>(W.icache);
+        for (unsigned i = lane; i < d.ins_len; i += 32) dst[i] = __ldg(src + i);
+        if (lane == 0) {
+          W.idef = d;
+          W.icache_def = id;
+        }
+      } else if (lane == 0) {
+        W.icache_def = ~0u;
+      }
+    }
     long long s0c = clock64();
     __syncwarp();
+    unsigned mine = 0;
     if (lane < n) {
-      L.ring_base = top;
-      L.ring_cap = unsigned(SCAP) - (top - bot);
-      L.interact(W.sel[2 * lane], W.sel[2 * lane + 1]);
-      L.settle();
+      long long l0 = clock64();
+      interact(c, W.sel[2 * lane], W.sel[2 * lane + 1]);
+      settle(c);
+      mine = unsigned(min(clock64() - l0, 0x7fffffffll));
     }
     __syncwarp();
-    if (lane == 0) {
-      W.st_busy += ull(clock64() - s0c);
-      W.st_lanes += n;
-      W.st_steps++;
+    {
+      unsigned mx = __reduce_max_sync(0xffffffffu, mine);
+      unsigned sm = __reduce_add_sync(0xffffffffu, mine);
+      if (lane == 0) {
+        W.st_busy += ull(clock64() - s0c);
+        W.st_lanes += n;
+        W.st_steps++;
+        W.st_lane_sum += sm;
+        W.st_lane_max += mx;
+      }
     }
     {
       unsigned pushed = min(W.ring_cnt, unsigned(SCAP) - (top - bot));
       top += pushed;
     }
     // Nodes reclaimed in this step become allocatable after a fence.
-    __threadfence();
+    mem_fence();
     __syncwarp();
     {
       int pn = max(W.pool_n, 0);
@@ -340,8 +377,8 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
       for (int i = mv + int(lane); i < fn; i += 32) {
         // pool full: the rest goes to this lane's overflow list
         ull node = W.freed[i];
-        L.store(node, L.ovf);
-        L.ovf = node;
+        st_gpu(heap_at(unsigned(cur), node), W.ovf[lane]);
+        W.ovf[lane] = node;
       }
       __syncwarp();
       if (lane == 0) {
@@ -362,17 +399,23 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
       // Give up to half the stack (at most four slots) per check.
       unsigned chunks = __shfl_sync(0xffffffffu, give, 0) ? min((top - bot) / 64u, 4u) : 0u;
       for (unsigned k = 0; k < chunks; k++) {
-        if (!donate(P, L, S, bot, 32u, cur, false)) break;
+        if (!donate(S, bot, 32u, cur, false)) break;
         if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
       }
     }
   }
-  if (cur >= 0) flush_counters(P, W, cur);
+  if (cur >= 0) flush_counters(W, cur);
   if (lane == 0) {
     atomicAdd(&C->stat_steps, W.st_steps);
     atomicAdd(&C->stat_lanes, W.st_lanes);
     atomicAdd(&C->stat_busy_cycles, W.st_busy);
     atomicAdd(&C->stat_idle_cycles, W.st_idle);
+    atomicAdd(&C->stat_lane_sum, W.st_lane_sum);
+    atomicAdd(&C->stat_lane_max, W.st_lane_max);
+    atomicAdd(&C->stat_total, ull(clock64() - born));
+#ifdef HVM_PROFILE_OPS
+    for (int k = 0; k < 8; k++) atomicAdd(&C->stat_prof[k], W.prof[k]);
+#endif
   }
 }
 
@@ -380,43 +423,44 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel(Params P) {
 // (Net::boot / Host::encode_net), then wrap the root in an expansion agent
 // (Net::expand, runtime/src/net.rs:65-69).  Redexes go to the global queue in
 // slots of up to 32.
-__global__ void boot_kernel(Params P, unsigned first, unsigned count) {
+__global__ void boot_kernel(unsigned first, unsigned count) {
   unsigned i = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= first + count) return;
   WarpSmem W;  // this thread's private copy (local memory)
   W.ring_cnt = 0;
+  W.icache_def = ~0u;
   W.pool_n = W.freed_n = 0;
-  for (int c = 0; c < NCOUNT; c++) W.rw[c] = 0;
-  Lane L(P, &W, 0);
-  L.net = i;
-  L.pool_cap = 0;
-  L.ring_base = 0;
-  L.ring_cap = CHUNK;
-  NetState& ns = P.nets[i];
-  ull root = L.alloc();
+  W.pool_cap = 0;
+  W.ring_base = 0;
+  W.ring_cap = CHUNK;
+  for (int k = 0; k < NCOUNT; k++) W.rw[k] = 0;
+  lane_init(&W, 0);
+  Ctx c{&W, 0, i};
+  NetState& ns = g_P.nets[i];
+  ull root = alloc(c);
   unsigned prog = unsigned(ns.prog);
-  if (prog < P.ndefs && !(P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
+  if (prog < g_P.ndefs && !(g_P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
   // Small Defs use register slots 0, 32, 64, ... of W.regs (lane 0's column).
-  L.run_def(prog, pvar(root));
-  L.settle();
-  root = L.expand(root);
-  L.settle();
+  run_def(c, prog, pvar(root));
+  settle(c);
+  root = expand(c, root);
+  settle(c);
   ns.root = root;
   unsigned k = min(W.ring_cnt, unsigned(CHUNK));
   if (k) {
     atomicAdd(reinterpret_cast<ull*>(&ns.pending), 1ull);
     ull pos;
-    if (q_reserve_push(P, L, pos, true)) {
-      Slot* s = &P.q[pos & P.ctrl->q_mask];
+    if (q_reserve_push(i, pos, true)) {
+      Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
       st_gpu(reinterpret_cast<ull*>(&s->net), (ull(k) << 32) | i);
       for (unsigned j = 0; j < 2 * k; j++) st_gpu(&s->r[j], W.stk[j]);
-      q_publish(P, pos);
+      q_publish(pos);
     }
   }
   for (int c = 0; c < NCOUNT; c++)
     if (W.rw[c]) atomicAdd(&ns.rw[c], W.rw[c]);
   __threadfence();
-  if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&P.ctrl->nets_left), 1ull);
+  if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&g_P.ctrl->nets_left), 1ull);
 }
 
 __global__ void queue_init_kernel(Slot* q, ull n) {
@@ -548,7 +592,8 @@ struct Runner {
   void launch(unsigned first, unsigned count, const hvm64_tuning& t, cudaStream_t st) {
     dev::Params p = params();
     unsigned bt = 128;
-    dev::boot_kernel<<<(count + bt - 1) / bt, bt, 0, st>>>(p, first, count);
+    CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, st));
+    dev::boot_kernel<<<(count + bt - 1) / bt, bt, 0, st>>>(first, count);
     CU(cudaGetLastError());
     CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             int(dev::SMEM_BYTES)));
@@ -559,7 +604,7 @@ struct Runner {
                                                        dev::SMEM_BYTES));
       bps = std::max(1, occ);
     }
-    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>(p);
+    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>();
     CU(cudaGetLastError());
   }
 
@@ -598,7 +643,7 @@ struct Runner {
 
     stat_donated = stat_spilled = stat_overflow = 0;
     stat_steps = stat_lanes = stat_busy = stat_idle = 0;
-    for (int k = 0; k < 8; k++) stat_g_steps[k] = stat_g_cycles[k] = 0;
+    for (int k = 0; k < 8; k++) stat_g_steps[k] = stat_g_cycles[k] = stat_prof[k] = 0;
     cudaStream_t st = 0;
     cudaEvent_t e0, e1;
     CU(cudaEventCreate(&e0));
@@ -634,10 +679,10 @@ struct Runner {
       stat_lanes += host_ctrl.stat_lanes;
       stat_busy += host_ctrl.stat_busy_cycles;
       stat_idle += host_ctrl.stat_idle_cycles;
-      for (int k = 0; k < 8; k++) {
-        stat_g_steps[k] += host_ctrl.stat_g_steps[k];
-        stat_g_cycles[k] += host_ctrl.stat_g_cycles[k];
-      }
+      for (int k = 0; k < 8; k++) stat_prof[k] += host_ctrl.stat_prof[k];
+      stat_g_steps[0] += host_ctrl.stat_lane_sum;
+      stat_g_steps[1] += host_ctrl.stat_lane_max;
+      stat_g_steps[2] += host_ctrl.stat_total;
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
       if (host_ctrl.error) {
         for (unsigned k = first; k < first + count; k++) host_nets[k].status = host_ctrl.error;
@@ -667,7 +712,7 @@ struct Runner {
   void set_deadline(cudaStream_t st, uint64_t timeout_ms);
   uint64_t stat_donated = 0, stat_spilled = 0, stat_overflow = 0, heap_used = 0;
   uint64_t stat_steps = 0, stat_lanes = 0, stat_busy = 0, stat_idle = 0;
-  uint64_t stat_g_steps[8] = {0}, stat_g_cycles[8] = {0};
+  uint64_t stat_g_steps[8] = {0}, stat_g_cycles[8] = {0}, stat_prof[8] = {0};
 
   void stats(hvm64_stats* o) const {
     *o = hvm64_stats{};
@@ -894,7 +939,7 @@ int hvm64_internal_class_steps(const hvm64_batch* b, uint64_t* steps8, uint64_t*
   if (!b) return HVM64_ERR_BAD_INPUT;
   for (int k = 0; k < 8; k++) {
     steps8[k] = b->r.stat_g_steps[k];
-    cycles8[k] = b->r.stat_g_cycles[k];
+    cycles8[k] = b->r.stat_prof[k];
   }
   return HVM64_OK;
 }

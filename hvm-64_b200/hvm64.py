@@ -15,7 +15,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "build", "libhvm64.so")
+LIB_PATH = os.environ.get("HVM64_LIB") or os.path.join(HERE, "build", "libhvm64.so")
 
 OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR = range(9)
 PERSISTENT, PLAIN = 0, 1

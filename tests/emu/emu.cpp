@@ -43,6 +43,9 @@ void flush(WarpSmem& W, NetState& ns) {
 std::unique_ptr<WarpSmem> new_warp() {
   auto W = std::make_unique<WarpSmem>();
   memset(W.get(), 0, sizeof(WarpSmem));
+  W->icache_def = ~0u;
+  W->pool_cap = POOL;
+  lane_init(W.get(), 0);
   return W;
 }
 
@@ -62,7 +65,7 @@ void give(Emu* E, WarpSmem& W, unsigned& bot, unsigned cnt, int cur) {
 void worker(Emu* E, unsigned share_min) {
   g_emu = E;
   auto W = new_warp();
-  Lane L(E->P, W.get(), 0);
+  Ctx c{W.get(), 0, 0};
   unsigned top = 0, bot = 0;
   int cur = -1;
   for (;;) {
@@ -86,13 +89,13 @@ void worker(Emu* E, unsigned share_min) {
       if (cur < 0) {
         if (ld_gpu64s(&E->C.nets_left) <= 0) break;
         if (globaltimer() > E->C.deadline) {
-          L.fail(HVM64_ERR_TIMEOUT, 1);
+          run_fail(c.net, HVM64_ERR_TIMEOUT, 1);
           break;
         }
         std::this_thread::yield();
         continue;
       }
-      L.net = unsigned(cur);
+      c.net = unsigned(cur);
       bot = 0;
       top = unsigned(got.size() / 2);
       for (size_t k = 0; k < got.size(); k++) W->stk[k] = got[k];
@@ -102,17 +105,17 @@ void worker(Emu* E, unsigned share_min) {
     ull a = W->stk[2 * i], b = W->stk[2 * i + 1];
     top -= 1;
     W->ring_cnt = 0;
-    L.ring_base = top;
-    L.ring_cap = unsigned(SCAP) - (top - bot);
-    L.interact(a, b);
-    L.settle();
+    W->ring_base = top;
+    W->ring_cap = unsigned(SCAP) - (top - bot);
+    interact(c, a, b);
+    settle(c);
     top += std::min(W->ring_cnt, unsigned(SCAP) - (top - bot));
     // merge reclaimed nodes into the pool
     int pn = std::max(W->pool_n, 0), fn = std::min(W->freed_n, POOL), mv = std::min(fn, POOL - pn);
     for (int k = 0; k < mv; k++) W->pool[pn + k] = W->freed[k];
     for (int k = mv; k < fn; k++) {
-      L.store(W->freed[k], L.ovf);
-      L.ovf = W->freed[k];
+      hstore(c, W->freed[k], W->ovf[0]);
+      W->ovf[0] = W->freed[k];
     }
     W->pool_n = pn + mv;
     W->freed_n = 0;
@@ -130,9 +133,9 @@ void worker(Emu* E, unsigned share_min) {
 }  // namespace
 
 // The emulation ships an overflowing redex to the shared queue.
-void hvm::dev::Lane::overflow_one(ull a, ull b) {
+void hvm::dev::push_overflow(unsigned net, ull a, ull b) {
   Emu* E = g_emu;
-  atom_add(reinterpret_cast<ull*>(&P.nets[net].pending), 1ull);
+  atom_add(reinterpret_cast<ull*>(&g_P.nets[net].pending), 1ull);
   std::lock_guard<std::mutex> g(E->mu);
   E->queue.push_back({net, std::vector<ull>{a, b}});
 }
@@ -165,19 +168,19 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     E.P.instrs = book.instrs.data();
     E.P.labbits = reinterpret_cast<const ull*>(book.labbits.data());
     E.P.ndefs = unsigned(book.defs.size());
+    g_P = E.P;
     // boot (the boot kernel's steps, one thread)
     g_emu = &E;
     {
       auto W = new_warp();
-      Lane L(E.P, W.get(), 0);
-      L.ring_cap = 0;  // boot redexes go straight to the shared queue
-      L.net = 0;
-      ull root = L.alloc();
+      W->ring_cap = 0;  // boot redexes go straight to the shared queue
+      Ctx c{W.get(), 0, 0};
+      ull root = alloc(c);
       if (!(book.defs[it->second].flags & 1)) W->rw[RW_DREF]++;
-      L.run_def(it->second, pvar(root));
-      L.settle();
-      root = L.expand(root);
-      L.settle();
+      run_def(c, it->second, pvar(root));
+      settle(c);
+      root = expand(c, root);
+      settle(c);
       E.nets[0].root = root;
       flush(*W, E.nets[0]);
       if (E.nets[0].pending > 0) E.C.nets_left = 1;
