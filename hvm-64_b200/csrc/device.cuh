@@ -34,10 +34,10 @@ namespace dev {
 
 typedef unsigned long long ull;
 
-constexpr int WARPS = 4;            // warps per reducer block
+constexpr int WARPS = 2;            // warps per reducer block
 constexpr int THREADS = WARPS * 32;
-constexpr int SCAP = 256;           // per-warp shared-memory redex stack (power of two)
-constexpr int HEADROOM = 128;       // stack slots kept free for the redexes of one step
+constexpr int SCAP = 512;           // per-warp shared-memory redex stack (power of two)
+constexpr int HEADROOM = 192;       // stack slots kept free for the redexes of one step
 constexpr int CHUNK = 32;           // redexes per global-queue slot
 constexpr int POOL = 64;            // per-warp pool of free nodes ready for reuse
 constexpr unsigned ICACHE = 32;     // instructions of the step's Def staged in shared memory
@@ -79,7 +79,7 @@ struct Ctrl {
   ull stat_steps, stat_lanes, stat_busy_cycles, stat_idle_cycles;
   ull timeout_ns;  // per launch: each warp's deadline is its start + timeout_ns
   ull stat_lane_sum, stat_lane_max, stat_total;  // per-lane interaction cycles (sum, per-step max), warp lifetime
-  ull stat_prof[8];  // profiling build: loads, exchanges, CAS (count, cycles), stores
+  ull stat_prof[32];  // profiling build: loads, exchanges, CAS (count, cycles), stores, per-rule cycles
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -158,6 +158,24 @@ __device__ __forceinline__ ull atom_add(ull* p, ull v) { return atomicAdd(p, v);
 __device__ __forceinline__ int atom_cas32(int* p, int e, int v) { return atomicCAS(p, e, v); }
 __device__ __forceinline__ unsigned atom_add_u32(unsigned* p, unsigned v) { return atomicAdd(p, v); }
 __device__ __forceinline__ int atom_add_i32(int* p, int v) { return atomicAdd(p, v); }
+// Warp-aggregated fetch-and-add of the same `v` by the converged lanes that
+// target the same word: one atomic per group, each lane gets its own offset
+// (lanes stepping in lock-step would otherwise serialise on the word).
+// Only shared memory qualifies: a local-memory word has the same generic
+// address in every thread.
+__device__ __forceinline__ int agg_add_i32(int* p, int v) {
+  if (!__isShared(p)) return atomicAdd(p, v);
+  unsigned mask = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(p));
+  unsigned ln = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (int(ln) == leader) base = atomicAdd(p, v * __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + v * __popc(mask & ((1u << ln) - 1u));
+}
+__device__ __forceinline__ unsigned agg_add_u32(unsigned* p, unsigned v) {
+  return unsigned(agg_add_i32(reinterpret_cast<int*>(p), int(v)));
+}
 // A release fence: the node fills and links before it are visible to any
 // lane that later reaches the node through a port published after it.
 __device__ __forceinline__ void mem_fence() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
@@ -213,6 +231,8 @@ inline int atom_cas32(int* p, int e, int v) {
 }
 inline unsigned atom_add_u32(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_add(v); }
 inline int atom_add_i32(int* p, int v) { return std::atomic_ref<int>(*p).fetch_add(v); }
+inline int agg_add_i32(int* p, int v) { return atom_add_i32(p, v); }
+inline unsigned agg_add_u32(unsigned* p, unsigned v) { return atom_add_u32(p, v); }
 inline void mem_fence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void pause_brief() { std::this_thread::yield(); }
 inline void lock_fill(ull* H, ull s, ull n) {
@@ -262,6 +282,7 @@ struct WarpSmem {
   DevDef idef;                // that Def's header
   unsigned icache_def;        // Def index staged in icache (~0u: none)
   ull rw[NCOUNT];             // counters of the warp's current net
+  unsigned cnt[NCOUNT * 32];  // per lane: counts of this step, [counter][lane] (folded into rw)
   ull ovf[32];                // per lane: overflow free list (left word links; right word LOCK)
   ull fw[4 * 32];             // per lane: words freed alone by the current interaction
   ull bnext[32], bend[32];    // per lane: pre-LOCKed bump chunk [bnext, bend), node indices
@@ -270,7 +291,7 @@ struct WarpSmem {
   unsigned ring_cap;          // ... for k < ring_cap
   int pool_cap;               // 0: no reuse pool (reclaimed nodes go to `ovf`)
 #ifdef HVM_PROFILE_OPS
-  ull prof[8];                // profiling build: op counts and wait cycles
+  ull prof[32];               // profiling build: op counts and wait cycles, cycles per rule
 #endif
   ull st_steps, st_lanes, st_busy, st_idle, st_lane_sum, st_lane_max, st_total;
   unsigned ring_cnt;
@@ -281,6 +302,7 @@ struct WarpSmem {
 
 // Initial per-lane / per-warp runtime state (lane `ln` of warp state `W`).
 HVM_INL void lane_init(WarpSmem* W, unsigned ln) {
+  for (int k = 0; k < NCOUNT; k++) W->cnt[k * 32 + ln] = 0;
   W->ovf[ln] = 0;
   for (int k = 0; k < 4; k++) W->fw[k * 32 + ln] = 0;
   W->bnext[ln] = W->bend[ln] = 0;
@@ -384,10 +406,34 @@ HVM_INL ull hload(const Ctx& c, ull a) {
   return ld_gpu(heap_at(c.net, a));
 #endif
 }
+#if defined(HVM_PROFILE_OPS) && defined(__CUDACC__)
+HVM_INL ull prof_done(const Ctx& c, int k, long long t, ull v) {
+  asm volatile("" : "+l"(v));
+  atomicAdd(&c.W->prof[k], 1ull);
+  atomicAdd(&c.W->prof[k + 1], ull(clock64() - t));
+  return v;
+}
+HVM_INL void hstore(const Ctx& c, ull a, ull v) {
+  atomicAdd(&c.W->prof[6], 1ull);
+  st_gpu(heap_at(c.net, a), v);
+}
+HVM_INL ull hswap(const Ctx& c, ull a, ull v) {
+  long long t = clock64();
+  return prof_done(c, 2, t, atom_exch(heap_at(c.net, a), v));
+}
+HVM_INL ull hcas(const Ctx& c, ull a, ull e, ull v) {
+  long long t = clock64();
+  return prof_done(c, 4, t, atom_cas(heap_at(c.net, a), e, v));
+}
+#define PROF_RULE(idx) long long prof_t0 = clock64(); struct ProfEnd { const Ctx& c; long long t; int k; \
+  __device__ ~ProfEnd() { atomicAdd(&c.W->prof[8 + 2 * k], 1ull); atomicAdd(&c.W->prof[9 + 2 * k], ull(clock64() - t)); } } prof_end{c, prof_t0, idx};
+#else
 HVM_INL void hstore(const Ctx& c, ull a, ull v) { st_gpu(heap_at(c.net, a), v); }
 HVM_INL ull hswap(const Ctx& c, ull a, ull v) { return atom_exch(heap_at(c.net, a), v); }
 HVM_INL ull hcas(const Ctx& c, ull a, ull e, ull v) { return atom_cas(heap_at(c.net, a), e, v); }
-HVM_INL void count(const Ctx& c, int k, ull v = 1) { atom_add(&c.W->rw[k], v); }
+#define PROF_RULE(k)
+#endif
+HVM_INL void count(const Ctx& c, int k, ull v = 1) { c.W->cnt[k * 32 + c.lane] += unsigned(v); }
 
 // wire.rs:342-350
 HVM_INL ull lock_target(const Ctx& c, ull w) {
@@ -405,7 +451,7 @@ HVM_INL ull lock_target(const Ctx& c, ull w) {
 // without reading the other half; otherwise the reference's store-FREE /
 // read-other-half / CAS sequence decides which lane reclaims.
 HVM_COLD void recycle(const Ctx& c, ull node) {
-  int k = c.W->pool_cap ? atom_add_i32(&c.W->freed_n, 1) : POOL;
+  int k = c.W->pool_cap ? agg_add_i32(&c.W->freed_n, 1) : POOL;
   if (k < c.W->pool_cap) {
     c.W->freed[k] = node;
   } else {
@@ -424,7 +470,7 @@ HVM_COLD ull alloc_slow(const Ctx& c) {
 HVM_INL ull alloc(const Ctx& c) {
   LS(allocs)++;
   if (c.W->pool_cap) {
-    int k = atom_add_i32(&c.W->pool_n, -1) - 1;
+    int k = agg_add_i32(&c.W->pool_n, -1) - 1;
     if (k >= 0) return c.W->pool[k];
   }
   ull b = LS(bnext);
@@ -452,6 +498,7 @@ HVM_COLD void claim(const Ctx& c, ull w, ull other) {
 // End of an interaction: look at the other half of every word freed alone
 // (the loads are in flight together).
 HVM_COLD void settle(const Ctx& c) {
+  PROF_RULE(6)
   ull w0 = FW(0), w1 = FW(1), w2 = FW(2), w3 = FW(3);
   if (!(w0 | w1 | w2 | w3)) return;
   ull o0 = w0 ? hload(c, w0 ^ 8) : 0, o1 = w1 ? hload(c, w1 ^ 8) : 0;
@@ -463,6 +510,7 @@ HVM_COLD void settle(const Ctx& c) {
   claim(c, w3, o3);
 }
 HVM_COLD void half_free(const Ctx& c, ull a) {
+  PROF_RULE(8)
   ull x = a ^ 8;
   int k = -1;
   if (a != 0) {
@@ -493,7 +541,7 @@ HVM_COLD void half_free(const Ctx& c, ull a) {
 // ---- redex pushes (linker.rs:70-85) -----------------------------------------
 HVM_INL void push(const Ctx& c, ull a, ull b) {
   unsigned cap = c.W->ring_cap;
-  unsigned k = cap ? atom_add_u32(&c.W->ring_cnt, 1u) : 0u;
+  unsigned k = cap ? agg_add_u32(&c.W->ring_cnt, 1u) : 0u;
   if (k < cap) {
     unsigned i = (c.W->ring_base + k) & unsigned(SCAP - 1);
     c.W->stk[2 * i] = a;
@@ -541,6 +589,7 @@ HVM_COLD void half_link_wire_port(const Ctx& c, ull ap, ull aw, ull bp) {
   }
 }
 HVM_COLD void link_wire_wire(const Ctx& c, ull aw, ull bw) {
+  PROF_RULE(9)
   ull ap = lock_target(c, aw);
   ull bp = lock_target(c, bw);
   if (principal(ap) && principal(bp)) {
@@ -554,6 +603,7 @@ HVM_COLD void link_wire_wire(const Ctx& c, ull aw, ull bw) {
 }
 // link_wire_port for a wire whose target `ap` was already taken (locked).
 HVM_COLD void link_locked_wire_port(const Ctx& c, ull aw, ull ap, ull bp) {
+  PROF_RULE(10)
   if (principal(ap) && principal(bp)) {
     half_free(c, aw);
     redux(c, ap, bp);
@@ -641,12 +691,14 @@ HVM_INL void link_taken(const Ctx& c, ull t, ull target, ull b) {
 
 // ---- rules (runtime/src/interact.rs) ------------------------------------------
 HVM_COLD void anni2(const Ctx& c, ull a, ull b) {  // interact.rs:72-79
+  PROF_RULE(0)
   count(c, RW_ANNI);
   ull a1 = paddr(a), b1 = paddr(b);
   link_wire_wire(c, a1, b1);
   link_wire_wire(c, a1 ^ 8, b1 ^ 8);
 }
 HVM_COLD void comm22(const Ctx& c, ull a, ull b) {  // interact.rs:118-141
+  PROF_RULE(1)
   count(c, RW_COMM);
   count(c, EX_COMM22);
   ull a1 = paddr(a), b1 = paddr(b);
@@ -662,12 +714,14 @@ HVM_COLD void comm22(const Ctx& c, ull a, ull b) {  // interact.rs:118-141
   link_wire_port(c, b1 ^ 8, mkport(ta, la, A2));
 }
 HVM_COLD void comm02(const Ctx& c, ull a, ull b) {  // interact.rs:162-168
+  PROF_RULE(2)
   count(c, RW_COMM);
   ull b1 = paddr(b);
   link_wire_port(c, b1, a);
   link_wire_port(c, b1 ^ 8, a);
 }
 HVM_COLD void switch_num(const Ctx& c, ull a, ull b) {  // interact.rs:201-223
+  PROF_RULE(3)
   count(c, RW_OPER);
   ull a1 = paddr(a);
   uint32_t num = uint32_t(b);
@@ -687,6 +741,7 @@ HVM_COLD void switch_num(const Ctx& c, ull a, ull b) {  // interact.rs:201-223
   }
 }
 HVM_COLD void op_num(const Ctx& c, ull a, ull b) {  // interact.rs:251-270
+  PROF_RULE(4)
   uint32_t op = plab(a);
   ull a1 = paddr(a);
   ull t1 = hload(c, a1);
@@ -705,6 +760,7 @@ HVM_COLD void op_num(const Ctx& c, ull a, ull b) {  // interact.rs:251-270
 
 // ---- instruction VM (runtime/src/instruction.rs:400-500, def.rs:217-289) -----
 HVM_COLD void do_ctr(const Ctx& c, unsigned lab, ull trg, ull& o1, ull& o2) {
+  PROF_RULE(11)
   ull port = trg_take(c, trg);
   if (ptag(port) == T_CTR && plab(port) == lab) {
     free_trg(c, trg);
@@ -823,6 +879,7 @@ HVM_COLD void exec_large(const Ctx& c, const DevDef& d, ull t0) {
   exec(c, d, t0, R, 1, g_P.instrs + d.ins_off);
 }
 HVM_COLD void run_def(const Ctx& c, unsigned id, ull t0) {
+  PROF_RULE(5)
   if (id >= g_P.ndefs) return run_fail(c.net, HVM64_ERR_BAD_INPUT, id);
   ull* R = c.W->regs + c.lane;
   if (id == c.W->icache_def) {  // staged by the warp for this step
@@ -906,6 +963,7 @@ HVM_COLD void call(const Ctx& c, ull port, ull trg) {
 
 // ---- interact.rs:6-44 ----------------------------------------------------------
 HVM_COLD void interact(const Ctx& c, ull a, ull b) {
+  PROF_RULE(7)
   unsigned at = ptag(a), bt = ptag(b);
   if (at <= T_VAR || bt <= T_VAR) return run_fail(c.net, HVM64_ERR_BAD_PAIR, a);
   bool an = at == T_REF || at == T_NUM, bn = bt == T_REF || bt == T_NUM;

@@ -128,10 +128,23 @@ __device__ bool donate(ull* S, unsigned& bot, unsigned cnt, int cur, bool must) 
   return true;
 }
 
+// Fold the lanes' per-step counts into the warp's counters.
+__device__ __forceinline__ void fold_counts(WarpSmem& W) {
+  const unsigned lane = threadIdx.x & 31;
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < NCOUNT; k++) {
+    unsigned v = __reduce_add_sync(0xffffffffu, W.cnt[k * 32 + lane]);
+    W.cnt[k * 32 + lane] = 0;
+    if (lane == 0 && v) W.rw[k] += v;
+  }
+  __syncwarp();
+}
+
 // Flush the warp's counters into its net (one atomic per counter).
 __device__ void flush_counters(WarpSmem& W, int cur) {
   const unsigned lane = threadIdx.x & 31;
-  __syncwarp();
+  fold_counts(W);
   if (lane < unsigned(NCOUNT)) {
     ull v = W.rw[lane];
     if (v) atomicAdd(&g_P.nets[cur].rw[lane], v);
@@ -141,9 +154,9 @@ __device__ void flush_counters(WarpSmem& W, int cur) {
 }
 
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
-static_assert(SMEM_BYTES <= 56 * 1024, "four reducer blocks per SM must fit in shared memory");
+static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
-__global__ void __launch_bounds__(THREADS, 4) reduce_kernel() {
+__global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
@@ -154,7 +167,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel() {
   lane_init(&W, lane);
   if (lane < unsigned(NCOUNT)) W.rw[lane] = 0;
 #ifdef HVM_PROFILE_OPS
-  if (lane < 8) W.prof[lane] = 0;
+  W.prof[lane] = 0;
 #endif
   if (lane == 0) {
     W.pool_n = 0;
@@ -366,6 +379,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel() {
       unsigned pushed = min(W.ring_cnt, unsigned(SCAP) - (top - bot));
       top += pushed;
     }
+    fold_counts(W);
     // Nodes reclaimed in this step become allocatable after a fence.
     mem_fence();
     __syncwarp();
@@ -414,7 +428,7 @@ __global__ void __launch_bounds__(THREADS, 4) reduce_kernel() {
     atomicAdd(&C->stat_lane_max, W.st_lane_max);
     atomicAdd(&C->stat_total, ull(clock64() - born));
 #ifdef HVM_PROFILE_OPS
-    for (int k = 0; k < 8; k++) atomicAdd(&C->stat_prof[k], W.prof[k]);
+    for (int k = 0; k < 32; k++) atomicAdd(&C->stat_prof[k], W.prof[k]);
 #endif
   }
 }
@@ -457,8 +471,10 @@ __global__ void boot_kernel(unsigned first, unsigned count) {
       q_publish(pos);
     }
   }
-  for (int c = 0; c < NCOUNT; c++)
-    if (W.rw[c]) atomicAdd(&ns.rw[c], W.rw[c]);
+  for (int k = 0; k < NCOUNT; k++) {
+    ull v = W.rw[k] + W.cnt[k * 32];
+    if (v) atomicAdd(&ns.rw[k], v);
+  }
   __threadfence();
   if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&g_P.ctrl->nets_left), 1ull);
 }
@@ -643,7 +659,8 @@ struct Runner {
 
     stat_donated = stat_spilled = stat_overflow = 0;
     stat_steps = stat_lanes = stat_busy = stat_idle = 0;
-    for (int k = 0; k < 8; k++) stat_g_steps[k] = stat_g_cycles[k] = stat_prof[k] = 0;
+    for (int k = 0; k < 8; k++) stat_g_steps[k] = stat_g_cycles[k] = 0;
+    for (int k = 0; k < 32; k++) stat_prof[k] = 0;
     cudaStream_t st = 0;
     cudaEvent_t e0, e1;
     CU(cudaEventCreate(&e0));
@@ -679,7 +696,7 @@ struct Runner {
       stat_lanes += host_ctrl.stat_lanes;
       stat_busy += host_ctrl.stat_busy_cycles;
       stat_idle += host_ctrl.stat_idle_cycles;
-      for (int k = 0; k < 8; k++) stat_prof[k] += host_ctrl.stat_prof[k];
+      for (int k = 0; k < 32; k++) stat_prof[k] += host_ctrl.stat_prof[k];
       stat_g_steps[0] += host_ctrl.stat_lane_sum;
       stat_g_steps[1] += host_ctrl.stat_lane_max;
       stat_g_steps[2] += host_ctrl.stat_total;
@@ -712,7 +729,7 @@ struct Runner {
   void set_deadline(cudaStream_t st, uint64_t timeout_ms);
   uint64_t stat_donated = 0, stat_spilled = 0, stat_overflow = 0, heap_used = 0;
   uint64_t stat_steps = 0, stat_lanes = 0, stat_busy = 0, stat_idle = 0;
-  uint64_t stat_g_steps[8] = {0}, stat_g_cycles[8] = {0}, stat_prof[8] = {0};
+  uint64_t stat_g_steps[8] = {0}, stat_g_cycles[8] = {0}, stat_prof[32] = {0};
 
   void stats(hvm64_stats* o) const {
     *o = hvm64_stats{};
@@ -935,12 +952,10 @@ int hvm64_batch_stats(const hvm64_batch* b, hvm64_stats* out) {
 }
 // Diagnostic (not in the public header): steps and cycles of the last run
 // by the number of distinct rule classes among the lanes of a step.
-int hvm64_internal_class_steps(const hvm64_batch* b, uint64_t* steps8, uint64_t* cycles8) {
+int hvm64_internal_class_steps(const hvm64_batch* b, uint64_t* steps8, uint64_t* prof32) {
   if (!b) return HVM64_ERR_BAD_INPUT;
-  for (int k = 0; k < 8; k++) {
-    steps8[k] = b->r.stat_g_steps[k];
-    cycles8[k] = b->r.stat_prof[k];
-  }
+  for (int k = 0; k < 8; k++) steps8[k] = b->r.stat_g_steps[k];
+  for (int k = 0; k < 32; k++) prof32[k] = b->r.stat_prof[k];
   return HVM64_OK;
 }
 

@@ -34,8 +34,10 @@ thread_local Emu* g_emu = nullptr;
 
 void flush(WarpSmem& W, NetState& ns) {
   for (int k = 0; k < NCOUNT; k++) {
-    if (W.rw[k]) atom_add(&ns.rw[k], W.rw[k]);
+    ull v = W.rw[k] + W.cnt[k * 32];
+    if (v) atom_add(&ns.rw[k], v);
     W.rw[k] = 0;
+    W.cnt[k * 32] = 0;
   }
 }
 
