@@ -9,10 +9,11 @@ reference's Rewrites::total) per second, in G/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank reduces its own batch (seeded by rank): weak scaling.
+Under torchrun each rank reduces its own batch (seeded by rank): weak scaling,
+no collective on the data path (the nets are independent).
 `--impl reference` times the CPU evaluator (the oracle's restatement of the
-reference's Net::parallel_normal, which cannot be built here) on a bounded
-sample of the same workload.
+reference's Net::parallel_normal; the Rust reference cannot be built without
+a Rust toolchain) on a bounded sample of the same workload.
 """
 import argparse
 import json
@@ -32,12 +33,26 @@ METRIC = "GInteractions/s on 1 B200, batched-persistent vs per-net plain; p99 la
 UNIT = "GInteractions/s"
 
 # Algorithmic bytes per interaction (HBM model: one port word = 8 B, an
-# exchange or CAS counts a read and a write; see DESIGN.md).
+# exchange or CAS counts a read and a write).
 BYTES = {"anni": 224, "comm22": 384, "comm02": 128, "eras": 0, "oper": 104}
 
+# DRAM bytes (read + write) per interaction of reduce_kernel: ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum (68.06 + 151.11 GB) over the
+# 1,414,382,623 interactions of one launch on a 4096-net batch of depth [8, 9]
+# (the full workload is too long to capture); scaled by the interactions of a
+# launch.
+TRAFFIC_PER_INTERACTION = (68.06e9 + 151.11e9) / 1414382623
 
-def dref_bytes(nodes, links):
-    return 32 + 40 * nodes + 32 * links
+
+def dref_bytes(nodes, links, calls):
+    return 32 * calls + 40 * nodes + 32 * links
+
+
+def algorithmic_bytes(counts, stats):
+    comm22 = stats["comm22"]
+    comm02 = counts["comm"] - comm22
+    return (counts["anni"] * BYTES["anni"] + comm22 * BYTES["comm22"] + comm02 * BYTES["comm02"] +
+            counts["oper"] * BYTES["oper"] + dref_bytes(stats["dref_nodes"], stats["dref_links"], counts["dref"]))
 
 
 def peaks():
@@ -46,6 +61,14 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def pow2_threads():
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    t = 1
+    while t * 2 <= n:
+        t *= 2
+    return t, n
 
 
 class Clocks:
@@ -83,8 +106,13 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if len(r) > 2 and num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if len(r) > 2 and num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in self.rows:
@@ -112,41 +140,39 @@ def cpu_baseline(entries, budget, threads):
         _, rw, s = oracle.run_book(text, entry=f"main_{j}", mode=oracle.MODE_PARALLEL, threads=threads)
         total += sum(rw.values())
         secs += s
-    desc = f"{len(sample)} of the batch's nets ({total} interactions), Net::parallel_normal restated, {threads} threads"
-    return total / secs / 1e9, desc, len(sample)
+    desc = (f"{len(sample)} of the batch's nets ({total} interactions): the C++ restatement of "
+            f"Net::parallel_normal, {threads} threads, timer around normal only")
+    return total / secs / 1e9, desc
+
+
+def config(args):
+    return {"workload": f"batched {args.nets} nets: tree-sum / bitonic-sort 50-50 by seed, depth log-uniform "
+                        f"[{args.dmin}, {args.dmax}], u24 keys",
+            "nets": args.nets, "dmin": args.dmin, "dmax": args.dmax, "mode": "persistent, one launch per step",
+            "l2": "flushed between steps (512 MiB write); heaps far above L2",
+            "parallelism": f"weak: {args.gpus} x 1 GPU, disjoint nets per rank"}
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    threads = os.cpu_count() or 1
-    t = 1
-    while t * 2 <= threads:
-        t *= 2
+    t, n = pow2_threads()
     entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=0)
     vals = []
     for step in range(args.warmup + args.steps):
-        v, desc, n = cpu_baseline(entries, args.cpu_budget, t)
+        v, desc = cpu_baseline(entries, args.cpu_budget / 4, t)
         if step >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": config(args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": t, "kind": "port", "sample": desc},
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": t, "kind": "port", "sample": desc,
+                         "host_cpus": n},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(out))
-
-
-def config(args):
-    return {"workload": f"batched {args.nets} nets: tree-sum / bitonic-sort 50-50, depth log-uniform "
-                        f"[{args.dmin}, {args.dmax}]",
-            "nets": args.nets, "dmin": args.dmin, "dmax": args.dmax, "mode": "persistent, one launch per step",
-            "l2": "flushed between steps (512 MiB write)", "parallelism": f"weak: {args.gpus} x 1 GPU"}
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -157,11 +183,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nets", type=int, default=4096)
     ap.add_argument("--dmin", type=int, default=8)
-    ap.add_argument("--dmax", type=int, default=12)
+    ap.add_argument("--dmax", type=int, default=14)
     ap.add_argument("--plain-nets", type=int, default=256, help="nets timed one-per-launch for the plain arm")
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=4e8, help="interactions in the CPU sample")
     ap.add_argument("--heap-gb", type=float, default=0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--device-only", action="store_true", help="skip the plain, e2e and CPU legs")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -176,7 +203,8 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
 
     import hvm64
     entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=rank)
@@ -190,19 +218,16 @@ def main():
 
     for _ in range(args.warmup):
         batch.normal(hvm64.PERSISTENT, tune)
-    # correctness of every net's normal form (outside the timed region)
-    bad = 0
-    for i, (kind, d, j) in enumerate(entries):
-        if not W.check_result(kind, d, j, batch.readback(i)):
-            bad += 1
+    # every net's normal form, checked outside the timed region
+    bad = sum(0 if W.check_result(kind, d, j, batch.readback(i)) else 1 for i, (kind, d, j) in enumerate(entries))
     total_per_step = sum(batch.rwts[i].total() for i in range(batch.n))
-    counts = {k: sum(getattr(batch.rwts[i], k) for i in range(batch.n)) for k in ("anni", "comm", "eras", "dref",
-                                                                                    "oper")}
+    counts = {k: sum(getattr(batch.rwts[i], k) for i in range(batch.n))
+              for k in ("anni", "comm", "eras", "dref", "oper")}
 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms = []
+    step_ms, kernel_ms = [], []
     with Clocks(local) as clk:
         for _ in range(args.steps):
             flush.fill_(1)
@@ -213,76 +238,100 @@ def main():
             e1.record()
             torch.cuda.synchronize()
             step_ms.append(e0.elapsed_time(e1))
+            kernel_ms.append(batch.device_ms)
     torch.cuda.synchronize()
     elapsed = sum(step_ms) / 1000.0
+    stats = batch.stats()
     if dist:
         t = torch.tensor([elapsed], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-        tot = torch.tensor([float(total_per_step)], device="cuda")
+        tot = torch.tensor([float(total_per_step)], device="cuda", dtype=torch.float64)
         dist.all_reduce(tot)
-        total_all = tot.item()
+        total_all = float(tot.item())
     else:
         total_all = float(total_per_step)
     value = total_all * args.steps / elapsed / 1e9
-    kernel_ms = statistics.mean(step_ms)
 
-    # plain arm: the first `plain_nets` nets, one launch each
-    plain_entries = entries[:args.plain_nets]
-    pbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
-    pbatch.normal(hvm64.PLAIN, tune)
-    ptotal = sum(pbatch.rwts[i].total() for i in range(pbatch.n))
-    p0 = time.perf_counter()
-    pbatch.normal(hvm64.PLAIN, tune)
-    plain_s = time.perf_counter() - p0
-    plain_value = ptotal / plain_s / 1e9
-    del pbatch
-
-    # e2e: public API from host memory: batch creation (tables to HBM), reduce,
-    # every net's normal form read back to host.
-    e0 = time.perf_counter()
-    ebatch = hvm64.Batch(book, names, heap)
-    ebatch.normal(hvm64.PERSISTENT, tune)
-    for i in range(ebatch.n):
-        ebatch.readback(i)
-    e2e_s = time.perf_counter() - e0
-    stats = ebatch.stats()
-    del ebatch
-
+    # roofline of reduce_kernel: algorithmic bytes of one launch over its
+    # device time (CUDA events the library records on its launching stream)
     hbm, peak_kind = peaks()
-    comm22 = stats.get("comm22", counts["comm"])
-    comm02 = counts["comm"] - comm22
-    alg = (counts["anni"] * BYTES["anni"] + comm22 * BYTES["comm22"] + comm02 * BYTES["comm02"] +
-           counts["oper"] * BYTES["oper"] + dref_bytes(stats.get("dref_nodes", 0), stats.get("dref_links", 0)) +
-           counts["dref"] * 0)
-    achieved = alg / (kernel_ms / 1000.0) / 1e9
+    alg = algorithmic_bytes(counts, stats)
+    kms = statistics.mean(kernel_ms)
+    achieved = alg / (kms / 1000.0) / 1e9
+    traffic = TRAFFIC_PER_INTERACTION * total_per_step if TRAFFIC_PER_INTERACTION else None
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": kernel_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args),
+        "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args),
         "interactions_per_step": total_per_step, "counts_per_step": counts, "nets_bad": bad,
-        "plain": {"value": plain_value, "unit": UNIT, "nets": len(plain_entries),
-                  "note": "one net per launch, wall time incl. launch + sync"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind},
-        "e2e": {"value": total_per_step / e2e_s / 1e9, "unit": UNIT,
-                "h2d_bytes_per_step": stats.get("h2d_bytes"), "d2h_bytes_per_step": stats.get("d2h_bytes")},
-        "device_stats": stats,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                     "kernel": "reduce_kernel (+ boot_kernel) device time per launch", "kernel_ms": kms,
+                     "algorithmic_bytes": alg},
         "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),
+        "device_stats": stats,
     }
-    if rank == 0 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        t = 1
-        while t * 2 <= threads:
-            t *= 2
-        v, desc, _ = cpu_baseline(entries, args.cpu_budget, t)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": t, "kind": "port", "sample": desc}
+
+    if not args.device_only:
+        # plain arm: the batch's first `plain_nets` nets, one launch each
+        plain_entries = entries[:args.plain_nets]
+        if plain_entries:
+            pbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
+            pbatch.normal(hvm64.PLAIN, tune)
+            ptotal = sum(pbatch.rwts[i].total() for i in range(pbatch.n))
+            torch.cuda.synchronize()
+            p0 = time.perf_counter()
+            pbatch.normal(hvm64.PLAIN, tune)
+            plain_s = time.perf_counter() - p0
+            pdev = pbatch.device_ms
+            del pbatch
+            # the batched reducer on the same subset, for the like-for-like ratio
+            sbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
+            sbatch.normal(hvm64.PERSISTENT, tune)
+            s0 = time.perf_counter()
+            sbatch.normal(hvm64.PERSISTENT, tune)
+            sub_s = time.perf_counter() - s0
+            del sbatch
+            out["plain"] = {"value": ptotal / plain_s / 1e9, "unit": UNIT, "nets": len(plain_entries),
+                            "device_value": ptotal / (pdev / 1000.0) / 1e9,
+                            "batched_same_nets": ptotal / sub_s / 1e9,
+                            "note": "one net per launch (wall time incl. launch + sync) vs the batched "
+                                    "reducer on the same nets, and the full batch's value"}
+
+        # e2e through the public API from host memory: tables and net list to
+        # the device, reduce, every net's normal form back to host text.
+        e2e_s, h2d, d2h = 0.0, 0, 0
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            e0 = time.perf_counter()
+            ebatch = hvm64.Batch(book, names, heap)
+            ebatch.normal(hvm64.PERSISTENT, tune)
+            for i in range(ebatch.n):
+                ebatch.readback(i)
+            e2e_s += time.perf_counter() - e0
+            st = ebatch.stats()
+            h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+            del ebatch
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        out["e2e"] = {"value": total_all * args.e2e_steps / e2e_s / 1e9, "unit": UNIT,
+                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                      "note": "Batch create + normal + readback of every net, wall clock"}
+
+        if rank == 0:
+            t, n = pow2_threads()
+            v, desc = cpu_baseline(entries, args.cpu_budget, t)
+            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": t, "kind": "port", "sample": desc,
+                                   "host_cpus": n}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps(out))
+        print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

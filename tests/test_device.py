@@ -32,3 +32,140 @@ def test_device_snapshot(prog):
     text, rw = hvm64.run_book(prog["source"], heap_bytes=1 << 30, tuning=t)
     assert text == prog["text"]
     assert rw == {k: prog[k] for k in ("anni", "comm", "eras", "dref", "oper")}
+
+
+# ---------------------------------------------------------------------------
+# Workload families (tree-sum, bitonic sort, Church) against the oracle
+# ---------------------------------------------------------------------------
+def _oracle():
+    from oracle import oracle
+    return oracle
+
+
+COUNTS = ("anni", "comm", "eras", "dref", "oper")
+
+
+@pytest.mark.gpu
+def test_batch_families_match_oracle():
+    """A ragged batch of tree-sum and bitonic nets in one persistent launch:
+    every net's normal form and counts equal the oracle's run of that net."""
+    import workloads as W
+    hvm64, oracle = _hvm(), _oracle()
+    entries = W.batch_entries(24, 4, 10, seed=3)
+    text = W.batch_book(entries)
+    batch = hvm64.Batch(hvm64.Book.from_str(text), [f"main_{j}" for _, _, j in entries], 1 << 30)
+    batch.normal(hvm64.PERSISTENT, hvm64.Tuning(timeout_ms=60000))
+    for i, (kind, d, j) in enumerate(entries):
+        want, want_rw, _ = oracle.run_book(text, entry=f"main_{j}")
+        got = batch.readback(i)
+        assert got == want, (kind, d, j)
+        assert batch.rwts[i].as_dict() == want_rw, (kind, d, j)
+        assert W.check_result(kind, d, j, got)
+
+
+@pytest.mark.gpu
+def test_plain_equals_persistent_and_repeats():
+    """One-net-per-launch and persistent runs give the same forms and
+    counts, and a second persistent run of the same batch repeats them."""
+    import workloads as W
+    hvm64 = _hvm()
+    entries = W.batch_entries(12, 4, 9, seed=5)
+    book = hvm64.Book.from_str(W.batch_book(entries))
+    names = [f"main_{j}" for _, _, j in entries]
+    runs = []
+    for mode in (hvm64.PLAIN, hvm64.PERSISTENT, hvm64.PERSISTENT):
+        b = hvm64.Batch(book, names, 1 << 30)
+        b.normal(mode, hvm64.Tuning(timeout_ms=60000))
+        runs.append([(b.readback(i), b.rwts[i].as_dict()) for i in range(b.n)])
+    assert runs[0] == runs[1] == runs[2]
+
+
+@pytest.mark.gpu
+def test_batch_expression_and_trivial_entries():
+    """Entries may be expression nets ('=' prefix), nets with no redex at
+    all, and Def boots, mixed in one batch."""
+    hvm64, oracle = _hvm(), _oracle()
+    src = "@two = (a (* a))\n@main = x & @two ~ (1 x)\n"
+    exprs = ["main", "=*", "=(a a)", "=x & 3 ~ $([+] $(4 x))", "two", "main"]
+    b = hvm64.Batch(hvm64.Book.from_str(src), exprs, 1 << 28)
+    b.normal(hvm64.PERSISTENT, hvm64.Tuning(timeout_ms=20000))
+    want_main, rw_main, _ = oracle.run_book(src, entry="main")
+    assert b.readback(0) == want_main and b.rwts[0].as_dict() == rw_main
+    assert b.readback(5) == want_main
+    for i in (1, 2, 3):  # expression nets: Host::encode_net, no boot call
+        want, want_rw = oracle.run_expr(src, exprs[i][1:])
+        assert b.readback(i) == want and b.rwts[i].as_dict() == want_rw
+    assert b.readback(1) == "*" and b.readback(2) == "(a a)" and b.readback(3) == "7"
+    want_two, rw_two, _ = oracle.run_book(src, entry="two")
+    assert b.readback(4) == want_two and b.rwts[4].as_dict() == rw_two
+
+
+@pytest.mark.gpu
+def test_tree_sum_depth18_full_size():
+    """The tree-sum workload at its full size (262,144 leaves): normal form is
+    the host-computed wrapping sum; counts equal the oracle's."""
+    import workloads as W
+    hvm64, oracle = _hvm(), _oracle()
+    text = W.tree_sum(18, 0)
+    got, rw = hvm64.run_book(text, heap_bytes=4 << 30, tuning=hvm64.Tuning(timeout_ms=60000))
+    assert got == str(W.expected_sum(18, 0))
+    _, want_rw, _ = oracle.run_book(text, mode=oracle.MODE_PARALLEL, threads=8)
+    assert rw == want_rw
+
+
+@pytest.mark.gpu
+def test_bitonic_depth15_sorted():
+    """Bitonic sort of 2^15 keys: the read-back leaves are the sorted input
+    multiset (size-independent check), counts equal the oracle's."""
+    import workloads as W
+    hvm64, oracle = _hvm(), _oracle()
+    text = W.bitonic(15, 2)
+    got, rw = hvm64.run_book(text, heap_bytes=4 << 30, tuning=hvm64.Tuning(timeout_ms=120000))
+    assert W.leaves(got) == sorted(W.sort_keys(15, 2))
+    _, want_rw, _ = oracle.run_book(text, mode=oracle.MODE_PARALLEL, threads=8)
+    assert rw == want_rw
+
+
+@pytest.mark.gpu
+def test_church_labels():
+    """The label-heavy Church net (numeral 2 with one DUP label per copy,
+    applied to itself 5 times, collapsed): normal form and counts equal the
+    oracle's."""
+    import workloads as W
+    hvm64, oracle = _hvm(), _oracle()
+    text = W.church(5)
+    want, want_rw, _ = oracle.run_book(text)
+    got, rw = hvm64.run_book(text, heap_bytes=1 << 30, tuning=hvm64.Tuning(timeout_ms=60000))
+    assert got == want
+    assert rw == want_rw
+
+
+# ---------------------------------------------------------------------------
+# Failure statuses: where the reference panics, the C ABI returns a code and
+# the context stays usable.  None of these faults the GPU: each ends in the
+# kernel's own checks (division, dispatch, allocator bound, run deadline).
+# ---------------------------------------------------------------------------
+ERROR_CASES = [
+    ("div0", "@main = x & 10 ~ $([/] $(0 x))\n", "ERR_DIV0", 1 << 26, 20000),
+    ("bad_pair", "@main = (a b) & ?(a b) ~ (c c)\n", "ERR_BAD_PAIR", 1 << 26, 20000),
+    ("oom", None, "ERR_OOM", 1 << 16, 20000),
+    ("timeout", "@L = (a b) & @L ~ (a b)\n@main = x & @L ~ (x *)\n", "ERR_TIMEOUT", 1 << 26, 300),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ERROR_CASES, ids=[c[0] for c in ERROR_CASES])
+def test_error_status(case):
+    import workloads as W
+    hvm64 = _hvm()
+    name, src, code, heap, timeout = case
+    if src is None:
+        src = W.tree_sum(12, 0)
+    net = hvm64.Net(hvm64.Book.from_str(src), heap)
+    net.boot("main")
+    with pytest.raises(hvm64.HvmError) as e:
+        net.normal(hvm64.Tuning(timeout_ms=timeout))
+    assert e.value.code == getattr(hvm64, code)
+    # the device is still usable afterwards
+    got, _ = hvm64.run_book("@main = x & 3 ~ $([*] $(5 x))\n", heap_bytes=1 << 24)
+    assert got == "15"
