@@ -966,3 +966,160 @@ int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Normalisation without device allocation (hvm64_net_normal_noalloc)
+// ===========================================================================
+// Every device buffer of this entry point -- control block, net record, redex
+// queue, Book tables and node heap -- is carved out of one file-scope array
+// that the library holds on every GPU that loads it, until the process exits.
+// In host code `g_noalloc_scratch` only names a host-side stand-in: its device
+// address comes from cudaGetSymbolAddress, taken once per device with that
+// device current, and every kernel is handed that address.
+namespace hvm {
+namespace noalloc {
+constexpr uint64_t SCRATCH_BYTES = uint64_t(64) << 20;  // 64 MiB in all
+constexpr unsigned QLOG2 = 12;                           // 4096 queue slots of 32 redexes
+constexpr uint64_t round_up(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+constexpr uint64_t OFF_CTRL = 0;
+constexpr uint64_t OFF_NET = round_up(OFF_CTRL + sizeof(dev::Ctrl));
+constexpr uint64_t OFF_QUEUE = round_up(OFF_NET + sizeof(dev::NetState));
+constexpr uint64_t OFF_BOOK = round_up(OFF_QUEUE + (uint64_t(1) << QLOG2) * sizeof(dev::Slot));
+constexpr uint64_t BOOK_BYTES = uint64_t(4) << 20;      // Def headers + instructions + label sets
+constexpr uint64_t OFF_HEAP = round_up(OFF_BOOK + BOOK_BYTES);
+constexpr uint64_t HEAP_BYTES = (SCRATCH_BYTES - OFF_HEAP) & ~uint64_t(15);
+static_assert(OFF_HEAP < SCRATCH_BYTES, "scratch layout");
+}  // namespace noalloc
+}  // namespace hvm
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[hvm::noalloc::SCRATCH_BYTES];
+
+namespace hvm {
+namespace noalloc {
+constexpr int MAX_DEVICES = 64;
+std::mutex g_setup_mu;
+unsigned char* g_dev_scratch[MAX_DEVICES] = {};
+
+// The device address of the scratch array on the current device (set-up on
+// the first call per device).
+unsigned char* scratch_here(int device) {
+  if (device < 0 || device >= MAX_DEVICES) throw Error(HVM64_ERR_CUDA, "device index out of range");
+  std::lock_guard<std::mutex> g(g_setup_mu);
+  if (!g_dev_scratch[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw Error(HVM64_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_dev_scratch[device] = static_cast<unsigned char*>(p);
+  }
+  return g_dev_scratch[device];
+}
+
+std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm64_rewrites* out) {
+  hvm64_tuning t{};
+  if (tp) t = *tp;
+  if (t.queue_slots_log2 && t.queue_slots_log2 != QLOG2)
+    throw Error(HVM64_ERR_BAD_INPUT, "the no-allocation entry point has a fixed queue of 2^12 slots "
+                                     "(queue_slots_log2 must be 0 or 12)");
+  auto it = book.ids.find(name);
+  if (it == book.ids.end()) throw Error(HVM64_ERR_BAD_INPUT, std::string("no definition named @") + name);
+  uint64_t defs_b = book.defs.size() * sizeof(DevDef), ins_b = book.instrs.size() * sizeof(DevInstr);
+  uint64_t lab_b = book.labbits.size() * 8;
+  uint64_t off_ins = round_up(defs_b), off_lab = off_ins + round_up(ins_b);
+  if (off_lab + lab_b > BOOK_BYTES)
+    throw Error(HVM64_ERR_BAD_INPUT, "Book too large for the no-allocation entry point: its device tables need " +
+                                         std::to_string(off_lab + lab_b) + " bytes, the limit is " +
+                                         std::to_string(BOOK_BYTES));
+  int device = 0, sms = 0;
+  CU(cudaGetDevice(&device));
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  unsigned char* base = scratch_here(device);
+  dev::Ctrl* ctrl = reinterpret_cast<dev::Ctrl*>(base + OFF_CTRL);
+  dev::NetState* ns = reinterpret_cast<dev::NetState*>(base + OFF_NET);
+  dev::Slot* q = reinterpret_cast<dev::Slot*>(base + OFF_QUEUE);
+  unsigned char* bk = base + OFF_BOOK;
+  dev::ull* heap = reinterpret_cast<dev::ull*>(base + OFF_HEAP);
+  cudaStream_t st = 0;
+
+  // The array keeps the previous call's contents: everything a run reads
+  // before writing is set here (control block, net record, queue sequence
+  // numbers, Book tables).  Heap nodes are LOCK-filled as they are handed out.
+  if (defs_b) CU(cudaMemcpyAsync(bk, book.defs.data(), defs_b, cudaMemcpyHostToDevice, st));
+  if (ins_b) CU(cudaMemcpyAsync(bk + off_ins, book.instrs.data(), ins_b, cudaMemcpyHostToDevice, st));
+  if (lab_b) CU(cudaMemcpyAsync(bk + off_lab, book.labbits.data(), lab_b, cudaMemcpyHostToDevice, st));
+  dev::NetState hn{};
+  hn.prog = int(it->second);
+  CU(cudaMemcpyAsync(ns, &hn, sizeof hn, cudaMemcpyHostToDevice, st));
+  uint64_t timeout_ms = t.timeout_ms ? t.timeout_ms : 120000;
+  dev::Ctrl c{};
+  c.bump = 1;
+  c.heap_nodes = HEAP_BYTES / 16;
+  c.heap_bytes = HEAP_BYTES;
+  c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
+  c.spin_limit = 1ull << 24;
+  c.donate_min = t.donate_min ? t.donate_min : 64;
+  c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+  c.q_mask = (1ull << QLOG2) - 1;
+  c.deadline = ~0ull;
+  c.timeout_ns = timeout_ms * 1000000ull;
+  CU(cudaMemcpyAsync(ctrl, &c, sizeof c, cudaMemcpyHostToDevice, st));
+  unsigned qn = 1u << QLOG2;
+  dev::queue_init_kernel<<<(qn + 255) / 256, 256, 0, st>>>(q, qn);
+  CU(cudaGetLastError());
+  dev::set_deadline_kernel<<<1, 1, 0, st>>>(ctrl, c.timeout_ns);
+  CU(cudaGetLastError());
+
+  dev::Params p{};
+  p.heap = heap;
+  p.heap_bytes = HEAP_BYTES;
+  p.ctrl = ctrl;
+  p.nets = ns;
+  p.nnets = 1;
+  p.q = q;
+  p.defs = reinterpret_cast<const DevDef*>(bk);
+  p.instrs = reinterpret_cast<const DevInstr*>(bk + off_ins);
+  p.labbits = reinterpret_cast<const dev::ull*>(bk + off_lab);
+  p.ndefs = unsigned(book.defs.size());
+  CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, st));
+  dev::boot_kernel<<<1, 128, 0, st>>>(0, 1);
+  CU(cudaGetLastError());
+  CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dev::SMEM_BYTES)));
+  int bps = int(t.blocks_per_sm);
+  if (bps <= 0) {
+    int occ = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
+    bps = std::max(1, occ);
+  }
+  dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>();
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(st));
+
+  dev::Ctrl hc{};
+  CU(cudaMemcpy(&hc, ctrl, sizeof hc, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(&hn, ns, sizeof hn, cudaMemcpyDeviceToHost));
+  if (hc.error) {
+    std::string msg = status_name(hc.error);
+    if (hc.error == HVM64_ERR_OOM)
+      msg += " (the no-allocation heap holds " + std::to_string(HEAP_BYTES / 16) + " nodes)";
+    throw Error(hc.error, msg);
+  }
+  if (out) *out = hvm64_rewrites{hn.rw[0], hn.rw[1], hn.rw[2], hn.rw[3], hn.rw[4]};
+  // Normal form: copy the used part of the heap to the host and read it back.
+  uint64_t used = std::min<uint64_t>(hc.bump, HEAP_BYTES / 16);
+  std::vector<uint64_t> image(used * 2);
+  CU(cudaMemcpy(image.data(), heap, used * 16, cudaMemcpyDeviceToHost));
+  std::string text;
+  with_big_stack([&] { text = readback(book, image.data(), image.size(), hn.root); });
+  return text;
+}
+}  // namespace noalloc
+}  // namespace hvm
+
+extern "C" int hvm64_net_normal_noalloc(const hvm64_book* book, const char* def_name, const hvm64_tuning* tuning,
+                                        hvm64_rewrites* out, char* buf, size_t cap, size_t* len) {
+  if (!book || !def_name) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  std::string s;
+  int rc = guarded([&] { s = hvm::noalloc::run(book->book, def_name, tuning, out); });
+  if (rc) return rc;
+  return copy_out(s, buf, cap, len);
+}

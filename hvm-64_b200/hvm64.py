@@ -25,7 +25,7 @@ EXPORTS = (
     "hvm64_last_error", "hvm64_version", "hvm64_book_load", "hvm64_book_def_count", "hvm64_book_def_name",
     "hvm64_book_free", "hvm64_net_create", "hvm64_net_boot", "hvm64_net_encode", "hvm64_net_normal",
     "hvm64_net_readback", "hvm64_net_free", "hvm64_batch_create", "hvm64_batch_normal", "hvm64_batch_readback",
-    "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats",
+    "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats", "hvm64_net_normal_noalloc",
 )
 
 
@@ -107,6 +107,8 @@ def lib(build_if_missing=True):
     L.hvm64_batch_free.argtypes = [P]
     L.hvm64_batch_stats.argtypes = [P, c.POINTER(Stats)]
     L.hvm64_net_stats.argtypes = [P, c.POINTER(Stats)]
+    L.hvm64_net_normal_noalloc.argtypes = [P, c.c_char_p, c.POINTER(Tuning), c.POINTER(Rewrites), c.c_char_p,
+                                           c.c_size_t, c.POINTER(c.c_size_t)]
     _lib = L
     return L
 
@@ -222,6 +224,20 @@ class Batch:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.hvm64_batch_free(self._h)
             self._h = None
+
+
+def normal_noalloc(book, entry="main", tuning=None, cap=1 << 20):
+    """hvm64_net_normal_noalloc: boot `entry`, normalise and read back using
+    only the library's built-in device array (no device allocation).
+    Returns (text, Rewrites)."""
+    rw = Rewrites()
+    buf = ctypes.create_string_buffer(cap)
+    n = ctypes.c_size_t()
+    t = ctypes.byref(tuning) if tuning is not None else None
+    _check(lib().hvm64_net_normal_noalloc(book._h, entry.encode(), t, ctypes.byref(rw), buf, cap, ctypes.byref(n)))
+    if n.value >= cap:
+        raise HvmError(ERR_BAD_INPUT, f"normal form needs {n.value + 1} bytes; pass a larger cap")
+    return buf.value.decode(), rw
 
 
 def run_book(text, entry="main", heap_bytes=0, tuning=None):

@@ -118,6 +118,33 @@ typedef struct hvm64_stats {
 int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
 int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
 
+/* Boot Def `def_name`, reduce it to normal form and read it back, without
+ * allocating any device memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a process where a framework's
+ * caching allocator or a memory pool has already reserved the device memory
+ * (a fresh cudaMalloc would fail or fragment it), a host under a fixed,
+ * audited device-memory budget, or a request loop that must not pay
+ * cudaMalloc's latency and implicit device-wide synchronisation per request.
+ * hvm64_net_create allocates a heap of its own; this call instead uses one
+ * array compiled into the library
+ * (64 MiB on every GPU that loads it, held until the process exits): a 4 MiB
+ * region for the Book's device tables, a 4096-slot redex queue and a heap of
+ * about 3.7 million nodes.  A Book whose tables exceed 4 MiB is refused with
+ * HVM64_ERR_BAD_INPUT, a net that outgrows the heap stops with HVM64_ERR_OOM,
+ * and tuning->queue_slots_log2 must be 0 or 12.  Host memory is used only to
+ * render the normal-form text.
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  Every call
+ * on a device shares the array and starts by resetting the parts a run reads
+ * (control block, net record, queue, Book tables), so calls that overlap on
+ * the GPU (from two host threads) race and must be serialised by the caller.
+ * Outputs: `out` (nullable) receives the Rewrites; the normal form is written
+ * as hvm64_net_readback writes it (buf/cap/len). */
+int hvm64_net_normal_noalloc(const hvm64_book* book, const char* def_name, const hvm64_tuning* tuning,
+                             hvm64_rewrites* out, char* buf, size_t cap, size_t* len);
+
 #ifdef __cplusplus
 }
 #endif
