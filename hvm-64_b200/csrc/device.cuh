@@ -80,17 +80,25 @@ struct Ctrl {
   ull timeout_ns;  // per launch: each warp's deadline is its start + timeout_ns
   ull stat_lane_sum, stat_lane_max, stat_total;  // per-lane interaction cycles (sum, per-step max), warp lifetime
   ull stat_prof[32];  // profiling build: loads, exchanges, CAS (count, cycles), stores, per-rule cycles
+  ull pad5[16];
+  ull req_head;       // serving: requests admitted so far
+  ull pad6[15];
+  ull req_tail;       // serving: requests the host has written (host copies, device reads)
+  int stop;           // serving: the host asks the reducer to end once idle
+  int pad7;
+  ull pad8[14];
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
 enum : int { EX_COMM22 = 5, EX_DNODES, EX_DLINKS };
 
-struct NetState {  // 96 bytes
+struct NetState {  // 112 bytes
   ull root;            // byte offset of the root wire
   long long pending;   // warps holding this net's work + queued chunks
   ull rw[NCOUNT];
   int prog;            // DevDef index of the boot program
   int status;
+  ull ticket, t_admit; // serving: the request running in this slot
 };
 
 struct Slot {  // 544 bytes: one chunk of up to 32 redexes of one net
@@ -99,6 +107,23 @@ struct Slot {  // 544 bytes: one chunk of up to 32 redexes of one net
   unsigned count;
   ull pad[2];
   ull r[2 * CHUNK];
+};
+
+// Serving: one request (host -> device) and one completion record (device ->
+// host).  Both live in page-locked host memory mapped into the device.
+struct ServeReq {  // 16 bytes
+  ull ticket;       // nonzero
+  unsigned slot;    // net slot the request runs in
+  unsigned prog;    // DevDef index of the Def to boot
+};
+struct ServeDone {  // 128 bytes; `ticket` is written last
+  ull ticket;
+  int status;
+  unsigned pairs;   // (address, word) pairs gathered into the slot's output
+  ull root;
+  ull rw[NCOUNT];
+  ull t_admit, t_done;  // %globaltimer, ns
+  ull pad[2];
 };
 
 struct Params {
@@ -112,6 +137,12 @@ struct Params {
   const DevInstr* __restrict__ instrs;
   const ull* __restrict__ labbits;
   unsigned ndefs;
+  // serving (all zero for a batch run)
+  unsigned serve;
+  const ServeReq* req;         // device ring of req_cap requests
+  ServeDone* done;             // per slot (mapped host memory)
+  ull* out;                    // per slot: out_cap (address, word) pairs (mapped host memory)
+  unsigned req_cap, out_cap;
 };
 
 // The run's parameters: CUDA constant memory (set before each launch), or a

@@ -677,10 +677,16 @@ struct Reader {
   std::unordered_map<uint64_t, size_t> vars;
   size_t next_var = 0;
   std::string o;
+  const std::unordered_map<uint64_t, uint64_t>* sparse = nullptr;  // gathered words, by address
 
   uint64_t load(uint64_t addr) const {
     uint64_t w = addr >> 3;
     if (w >= words) throw Error(HVM64_ERR_BAD_INPUT, "readback: address outside the heap");
+    if (sparse) {
+      auto it = sparse->find(addr);
+      if (it == sparse->end()) throw Error(HVM64_ERR_BAD_INPUT, "readback: word not gathered");
+      return it->second;
+    }
     return heap[w];
   }
   bool live_addr(uint64_t p) const { return (p >> 48) == 0 && (p & ADDR_MASK) != 0 && ((p & ADDR_MASK) >> 3) < words; }
@@ -759,6 +765,17 @@ struct Reader {
 
 std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root) {
   Reader r{book, heap, heap_words, {}, 0, {}};
+  r.wire(root);
+  return r.o;
+}
+
+std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npairs, uint64_t heap_words,
+                           uint64_t root) {
+  std::unordered_map<uint64_t, uint64_t> m;
+  m.reserve(npairs * 2);
+  for (size_t i = 0; i < npairs; i++) m[pairs[2 * i]] = pairs[2 * i + 1];
+  Reader r{book, nullptr, heap_words, {}, 0, {}};
+  r.sparse = &m;
   r.wire(root);
   return r.o;
 }

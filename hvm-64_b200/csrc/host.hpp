@@ -129,6 +129,9 @@ struct Book {
 // (Host::readback, host/src/readback.rs:23-87).  Redirect chains (Red ports
 // left by concurrent linking) are followed to the live endpoint.
 std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root);
+// The same from the (address, word) pairs a serving reducer gathered.
+std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npairs, uint64_t heap_words,
+                           uint64_t root);
 
 // Runs f on a thread with a large stack (deep trees recurse; the reference
 // grows its stack with `stacker`, util/src/maybe_grow.rs).

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <memory>
 #include <mutex>
@@ -153,6 +154,134 @@ __device__ void flush_counters(WarpSmem& W, int cur) {
   __syncwarp();
 }
 
+// ---- serving -------------------------------------------------------------------
+// A served net's normal form leaves the device as the (address, word) pairs
+// that host readback (host/src/readback.rs:23-87) would load: the root word,
+// both words of every node it reaches, and each redirect chain a Var goes
+// through.  Lane 0 walks it depth-first, using the warp's redex ring (empty
+// when a net completes) as its stack, and writes the pairs into the slot's
+// output in mapped host memory.
+__device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull root, int& status) {
+  ull* out = g_P.out + ull(slot) * g_P.out_cap * 2;
+  const unsigned cap = g_P.out_cap;
+  const ull hb = g_P.heap_bytes;
+  ull* stk = W.stk;
+  const unsigned scap = 2 * SCAP;
+  unsigned sp = 0, n = 0;
+  auto emit = [&](ull w, ull v) {
+    if (n < cap) {
+      out[2 * n] = w;
+      out[2 * n + 1] = v;
+    }
+    n++;
+  };
+  auto live = [&](ull p) {
+    ull a = p & A_MASK;
+    return (p >> 48) == 0 && a != 0 && a < hb;
+  };
+  stk[sp++] = root;
+  while (sp) {
+    ull w = stk[--sp];
+    ull v = ld_gpu(heap_at(slot, w));
+    emit(w, v);
+    unsigned t = unsigned(v & 7);
+    if (t == T_VAR || t == T_RED) {
+      if (live(v)) {
+        ull e = paddr(v);
+        for (unsigned g = 0; g < (1u << 20); g++) {
+          ull x = ld_gpu(heap_at(slot, e));
+          emit(e, x);
+          if ((x & 7) != T_RED || !live(x)) break;
+          e = paddr(x);
+        }
+      }
+    } else if (t == T_OP || t == T_CTR || t == T_SWITCH) {
+      if (sp + 2 > scap) {
+        status = HVM64_ERR_OUTPUT;
+        break;
+      }
+      ull a = paddr(v);
+      stk[sp++] = a ^ 8;
+      stk[sp++] = a;
+    }
+    if (n > cap) {
+      status = HVM64_ERR_OUTPUT;
+      break;
+    }
+  }
+  return n < cap ? n : cap;
+}
+
+// The net in `slot` reached normal form: gather it and post its completion
+// record (the ticket last, after a system-scope fence).  Lane 0 only.
+__device__ __noinline__ void serve_complete(WarpSmem& W, unsigned slot) {
+  __threadfence();
+  NetState& ns = g_P.nets[slot];
+  int status = ld_gpu32(&ns.status);
+  if (ld_gpu32(&g_P.ctrl->error)) status = ld_gpu32(&g_P.ctrl->error);
+  ull root = ld_gpu(&ns.root);
+  unsigned n = serve_gather(W, slot, root, status);
+  volatile ServeDone* d = g_P.done + slot;
+  d->status = status;
+  d->pairs = n;
+  d->root = root;
+  for (int k = 0; k < NCOUNT; k++) d->rw[k] = ld_gpu(&ns.rw[k]);
+  d->t_admit = ld_gpu(&ns.t_admit);
+  d->t_done = globaltimer();
+  __threadfence_system();
+  d->ticket = ld_gpu(&ns.ticket);
+  __threadfence_system();
+}
+
+// Take the next request, if the host has written one, and boot it in this
+// warp: its first redexes land in the (empty) ring.  Lane 0 only; returns the
+// slot + 1, or 0.
+__device__ __noinline__ unsigned serve_admit(WarpSmem& W, Ctx& c) {
+  Ctrl* C = g_P.ctrl;
+  ull t = ld_gpu(&C->req_tail);
+  ull h = ld_gpu(&C->req_head);
+  bool got = false;
+  while (h < t) {
+    ull old = atomicCAS(&C->req_head, h, h + 1);
+    if (old == h) {
+      got = true;
+      break;
+    }
+    h = old;
+  }
+  if (!got) return 0;
+  mem_fence();
+  const ServeReq* r = g_P.req + (h % g_P.req_cap);
+  ull ticket = ld_gpu(&r->ticket);
+  ull sp = ld_gpu(reinterpret_cast<const ull*>(&r->slot));
+  unsigned slot = unsigned(sp), prog = unsigned(sp >> 32);
+  if (slot >= g_P.nnets) {
+    run_fail(0, HVM64_ERR_BAD_INPUT, slot);
+    return 0;
+  }
+  NetState& ns = g_P.nets[slot];
+  for (int k = 0; k < NCOUNT; k++) st_gpu(&ns.rw[k], 0);
+  st_gpu(reinterpret_cast<ull*>(&ns.pending), 1);  // this warp holds the new net
+  ns.prog = int(prog);
+  ns.status = 0;
+  st_gpu(&ns.ticket, ticket);
+  st_gpu(&ns.t_admit, globaltimer());
+  mem_fence();
+  atomicAdd(reinterpret_cast<ull*>(&C->nets_left), 1ull);
+  c.net = slot;
+  W.ring_base = 0;
+  W.ring_cap = unsigned(SCAP - HEADROOM);
+  W.ring_cnt = 0;
+  ull root = alloc(c);
+  if (prog < g_P.ndefs && !(g_P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
+  run_def(c, prog, pvar(root));
+  settle(c);
+  root = expand(c, root);
+  settle(c);
+  st_gpu(&ns.root, root);
+  return slot + 1;
+}
+
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
@@ -201,10 +330,15 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
     if (top == bot) {
       if (cur >= 0) {
         flush_counters(W, cur);
+        int fin = 0;
         if (lane == 0) {
+          if (g_P.serve) __threadfence();  // this warp's heap writes, before its share is released
           long long old = (long long)atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), ~0ull);
-          if (old == 1) atomicAdd(reinterpret_cast<ull*>(&C->nets_left), ~0ull);
+          fin = old == 1;
+          if (fin && g_P.serve) serve_complete(W, unsigned(cur));
+          if (fin) atomicAdd(reinterpret_cast<ull*>(&C->nets_left), ~0ull);
         }
+        __syncwarp();
         cur = -1;
       }
       ull pos = 0;
@@ -215,10 +349,23 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
         // Idle: back off exponentially (1 us .. 64 us) so that waiting warps
         // do not crowd the queue's and the counters' L2 lines.
         int stop = 0;
+        unsigned admitted = 0;
         if (lane == 0) {
           if (!hungry) atomicAdd(reinterpret_cast<ull*>(&C->hungry), 1ull);
-          if (ld_gpu64s(&C->nets_left) <= 0) stop = 1;
-          else if ((++idle & 15) == 0 && globaltimer() > deadline) {
+          if (g_P.serve) {
+            // Serving: boot the next request here, or end once the host has
+            // asked to stop and nothing is admitted, queued or running.
+            admitted = serve_admit(W, c);
+            if (!admitted && ld_gpu32(&C->stop) && ld_gpu64s(&C->nets_left) <= 0 &&
+                ld_gpu(&C->req_head) >= ld_gpu(&C->req_tail))
+              stop = 1;
+            else if (!admitted && (++idle & 15) == 0 && globaltimer() > deadline) {
+              run_fail(0, HVM64_ERR_TIMEOUT, 3);  // a server lives at most timeout_ms
+              stop = 1;
+            }
+          } else if (ld_gpu64s(&C->nets_left) <= 0) {
+            stop = 1;
+          } else if ((++idle & 15) == 0 && globaltimer() > deadline) {
             run_fail(0, HVM64_ERR_TIMEOUT, 1);
             stop = 1;
           }
@@ -226,7 +373,20 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
         }
         hungry = true;
         if (__shfl_sync(0xffffffffu, stop, 0)) break;
-        nap = nap ? min(nap * 2, 65536u) : 1024u;
+        admitted = __shfl_sync(0xffffffffu, admitted, 0);
+        if (admitted) {
+          if (lane == 0) atomicAdd(reinterpret_cast<ull*>(&C->hungry), ~0ull);
+          hungry = false;
+          nap = 0;
+          idle = 0;
+          cur = int(admitted - 1);
+          c.net = unsigned(cur);
+          bot = 0;
+          top = min(W.ring_cnt, unsigned(SCAP - HEADROOM));
+          continue;
+        }
+        // (a serving reducer naps at most 8 us: new requests wait on it)
+        nap = nap ? min(nap * 2, g_P.serve ? 8192u : 65536u) : 1024u;
         long long t0 = clock64();
         __nanosleep(nap);
         if (lane == 0) W.st_idle += ull(clock64() - t0);
@@ -533,6 +693,7 @@ const char* status_name(int s) {
     case HVM64_ERR_CUDA: return "CUDA error";
     case HVM64_ERR_QUEUE: return "device redex queue overflow";
     case HVM64_ERR_BAD_ADDR: return "heap address outside the arena";
+    case HVM64_ERR_OUTPUT: return "normal form larger than the request's output buffer";
   }
   return "unknown error";
 }
@@ -778,6 +939,223 @@ void Runner::set_deadline(cudaStream_t st, uint64_t timeout_ms) {
   CU(cudaGetLastError());
 }
 
+
+// ===========================================================================
+// Serving: one persistent reducer that admits requests while it runs
+// ===========================================================================
+// The reducer kernel runs until the host stops it.  The host writes requests
+// (Def to boot, slot) into a device ring and bumps the ring's tail with async
+// copies on a second stream; an idle warp takes a request, boots it in its
+// own stack and reduces it alongside everything else in flight.  When a net's
+// last holder lets it go, that warp gathers its normal form into the slot's
+// output and posts a completion record, both in mapped host memory, which the
+// host polls.  Slots bound the nets in flight; the heap is shared and only
+// grows (normal forms stay until the server is freed).
+struct Server {
+  Book book;
+  int device = 0, sms = 148;
+  uint64_t heap_bytes = 0;
+  unsigned nslots = 0, out_cap = 0, req_cap = 0;
+  DevBuf<dev::ull> heap;
+  DevBuf<dev::Ctrl> ctrl;
+  DevBuf<dev::NetState> nets;
+  DevBuf<dev::Slot> q;
+  DevBuf<DevDef> d_defs;
+  DevBuf<DevInstr> d_instrs;
+  DevBuf<dev::ull> d_labbits;
+  DevBuf<dev::ServeReq> req;
+  dev::ServeDone* done = nullptr;  // mapped host memory
+  dev::ull* out = nullptr;         // mapped host memory
+  dev::ServeReq* req_stage = nullptr;  // pinned staging for the async copies
+  uint64_t* tail_stage = nullptr;
+  int* stop_stage = nullptr;
+  cudaStream_t ks = nullptr, cs = nullptr;
+  bool running = false;
+  uint64_t tail = 0, next_ticket = 1;
+  std::vector<uint64_t> slot_ticket;  // 0: free
+  std::vector<unsigned> free_slots;
+
+  ~Server() { shutdown(); }
+
+  void start(uint64_t bytes, unsigned slots, unsigned out_pairs, const hvm64_tuning& t) {
+    CU(cudaGetDevice(&device));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    if (slots == 0 || slots > (1u << 20)) throw Error(HVM64_ERR_BAD_INPUT, "slots must be in 1..2^20");
+    if (out_pairs == 0) throw Error(HVM64_ERR_BAD_INPUT, "out_pairs must be > 0");
+    if (bytes == 0) {
+      size_t fr = 0, tot = 0;
+      CU(cudaMemGetInfo(&fr, &tot));
+      bytes = std::min<uint64_t>(uint64_t(fr) / 2, uint64_t(16) << 30);
+    }
+    heap_bytes = bytes & ~uint64_t(15);
+    nslots = slots;
+    out_cap = out_pairs;
+    req_cap = 2 * slots + 16;
+    unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : 16;
+    if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
+    size_t qn = size_t(1) << qlog2;
+    heap.alloc(heap_bytes / 8);
+    ctrl.alloc(1);
+    nets.alloc(nslots);
+    q.alloc(qn);
+    req.alloc(req_cap);
+    d_defs.alloc(book.defs.size());
+    d_instrs.alloc(book.instrs.size());
+    d_labbits.alloc(book.labbits.size());
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&done), sizeof(dev::ServeDone) * nslots, cudaHostAllocMapped));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&out), sizeof(dev::ull) * 2 * size_t(out_cap) * nslots,
+                     cudaHostAllocMapped));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&req_stage), sizeof(dev::ServeReq) * req_cap, cudaHostAllocDefault));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&tail_stage), sizeof(uint64_t) * req_cap, cudaHostAllocDefault));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&stop_stage), sizeof(int), cudaHostAllocDefault));
+    memset(done, 0, sizeof(dev::ServeDone) * nslots);
+    *stop_stage = 0;
+    dev::ServeDone* d_done = nullptr;
+    dev::ull* d_out = nullptr;
+    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_done), done, 0));
+    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_out), out, 0));
+    CU(cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    if (!book.defs.empty())
+      CU(cudaMemcpyAsync(d_defs.p, book.defs.data(), book.defs.size() * sizeof(DevDef), cudaMemcpyHostToDevice, ks));
+    if (!book.instrs.empty())
+      CU(cudaMemcpyAsync(d_instrs.p, book.instrs.data(), book.instrs.size() * sizeof(DevInstr),
+                         cudaMemcpyHostToDevice, ks));
+    if (!book.labbits.empty())
+      CU(cudaMemcpyAsync(d_labbits.p, book.labbits.data(), book.labbits.size() * 8, cudaMemcpyHostToDevice, ks));
+    CU(cudaMemsetAsync(nets.p, 0, sizeof(dev::NetState) * nslots, ks));
+    dev::Ctrl c{};
+    c.bump = 1;
+    c.heap_nodes = heap_bytes / 16;
+    c.heap_bytes = heap_bytes;
+    c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
+    c.spin_limit = 1ull << 24;
+    c.donate_min = t.donate_min ? t.donate_min : 64;
+    c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+    c.q_mask = qn - 1;
+    c.deadline = ~0ull;
+    // a server runs until stopped, or until its lifetime (timeout_ms) ends
+    c.timeout_ns = (t.timeout_ms ? t.timeout_ms : 600000ull) * 1000000ull;
+    CU(cudaMemcpyAsync(ctrl.p, &c, sizeof c, cudaMemcpyHostToDevice, ks));
+    dev::queue_init_kernel<<<unsigned((qn + 255) / 256), 256, 0, ks>>>(q.p, qn);
+    CU(cudaGetLastError());
+    dev::Params p{};
+    p.heap = heap.p;
+    p.heap_bytes = heap_bytes;
+    p.ctrl = ctrl.p;
+    p.nets = nets.p;
+    p.nnets = nslots;
+    p.q = q.p;
+    p.defs = d_defs.p;
+    p.instrs = d_instrs.p;
+    p.labbits = d_labbits.p;
+    p.ndefs = unsigned(book.defs.size());
+    p.serve = 1;
+    p.req = req.p;
+    p.done = d_done;
+    p.out = d_out;
+    p.req_cap = req_cap;
+    p.out_cap = out_cap;
+    CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, ks));
+    CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(dev::SMEM_BYTES)));
+    int bps = int(t.blocks_per_sm);
+    if (bps <= 0) {
+      int occ = 0;
+      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
+      bps = std::max(1, occ);
+    }
+    CU(cudaStreamSynchronize(ks));  // tables and parameters in place before the reducer starts
+    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, ks>>>();
+    CU(cudaGetLastError());
+    running = true;
+    slot_ticket.assign(nslots, 0);
+    free_slots.clear();
+    for (unsigned i = nslots; i-- > 0;) free_slots.push_back(i);
+  }
+
+  // Nonzero when the reducer stopped on an error (read without waiting).
+  int device_error() {
+    int e = 0;
+    if (cudaStreamQuery(ks) == cudaSuccess) {
+      dev::Ctrl h{};
+      CU(cudaMemcpy(&h, ctrl.p, sizeof h, cudaMemcpyDeviceToHost));
+      e = h.error;
+    }
+    return e;
+  }
+
+  uint64_t submit(const std::string& name) {
+    if (!running) throw Error(HVM64_ERR_BAD_INPUT, "server is not running");
+    auto it = book.ids.find(name);
+    if (it == book.ids.end()) throw Error(HVM64_ERR_BAD_INPUT, "no definition named @" + name);
+    if (free_slots.empty()) throw Error(HVM64_ERR_QUEUE, "no free slot: poll and collect results first");
+    unsigned slot = free_slots.back();
+    free_slots.pop_back();
+    uint64_t ticket = next_ticket++;
+    slot_ticket[slot] = ticket;
+    unsigned k = unsigned(tail % req_cap);
+    req_stage[k] = dev::ServeReq{ticket, slot, it->second};
+    CU(cudaMemcpyAsync(req.p + k, req_stage + k, sizeof(dev::ServeReq), cudaMemcpyHostToDevice, cs));
+    tail_stage[k] = ++tail;
+    CU(cudaMemcpyAsync(&ctrl.p->req_tail, tail_stage + k, 8, cudaMemcpyHostToDevice, cs));
+    CU(cudaStreamSynchronize(cs));
+    return ticket;
+  }
+
+  size_t poll(uint64_t* tickets, size_t cap) {
+    size_t n = 0;
+    for (unsigned s = 0; s < nslots && n < cap; s++) {
+      uint64_t t = slot_ticket[s];
+      if (t && reinterpret_cast<volatile dev::ServeDone*>(done + s)->ticket == t) tickets[n++] = t;
+    }
+    return n;
+  }
+
+  int result(uint64_t ticket, hvm64_rewrites* rw, double* latency_us, std::string& text) {
+    unsigned s = 0;
+    while (s < nslots && slot_ticket[s] != ticket) s++;
+    if (s == nslots) throw Error(HVM64_ERR_BAD_INPUT, "unknown or collected ticket");
+    volatile dev::ServeDone* d = done + s;
+    if (d->ticket != ticket) throw Error(HVM64_ERR_BAD_INPUT, "request not finished yet");
+    std::atomic_thread_fence(std::memory_order_acquire);
+    int status = d->status;
+    if (rw) *rw = hvm64_rewrites{d->rw[0], d->rw[1], d->rw[2], d->rw[3], d->rw[4]};
+    if (latency_us) *latency_us = double(d->t_done - d->t_admit) / 1000.0;
+    if (status == 0) {
+      std::vector<uint64_t> pairs(2 * size_t(d->pairs));
+      memcpy(pairs.data(), out + 2 * size_t(out_cap) * s, pairs.size() * 8);
+      uint64_t root = d->root;
+      with_big_stack([&] { text = readback_pairs(book, pairs.data(), d->pairs, heap_bytes / 8, root); });
+    }
+    slot_ticket[s] = 0;
+    free_slots.push_back(s);
+    return status;
+  }
+
+  void shutdown() {
+    if (running) {
+      *stop_stage = 1;
+      cudaMemcpyAsync(&ctrl.p->stop, stop_stage, sizeof(int), cudaMemcpyHostToDevice, cs);
+      cudaStreamSynchronize(cs);
+      cudaStreamSynchronize(ks);
+      running = false;
+    }
+    if (ks) cudaStreamDestroy(ks);
+    if (cs) cudaStreamDestroy(cs);
+    ks = cs = nullptr;
+    if (done) cudaFreeHost(done);
+    if (out) cudaFreeHost(out);
+    if (req_stage) cudaFreeHost(req_stage);
+    if (tail_stage) cudaFreeHost(tail_stage);
+    if (stop_stage) cudaFreeHost(stop_stage);
+    done = nullptr;
+    out = nullptr;
+    req_stage = nullptr;
+    tail_stage = nullptr;
+    stop_stage = nullptr;
+  }
+};
 }  // namespace hvm
 
 // ===========================================================================
@@ -1123,3 +1501,51 @@ extern "C" int hvm64_net_normal_noalloc(const hvm64_book* book, const char* def_
   if (rc) return rc;
   return copy_out(s, buf, cap, len);
 }
+
+struct hvm64_server {
+  hvm::Server s;
+};
+
+extern "C" {
+
+int hvm64_server_create(const hvm64_book* book, uint64_t heap_bytes, uint32_t slots, uint32_t out_pairs,
+                        const hvm64_tuning* tuning, hvm64_server** out) {
+  if (!book || !out) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] {
+    auto sv = std::make_unique<hvm64_server>();
+    sv->s.book = book->book;
+    hvm64_tuning t{};
+    if (tuning) t = *tuning;
+    sv->s.start(heap_bytes, slots, out_pairs, t);
+    *out = sv.release();
+  });
+}
+int hvm64_server_submit(hvm64_server* sv, const char* def_name, uint64_t* ticket) {
+  if (!sv || !def_name || !ticket) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] { *ticket = sv->s.submit(def_name); });
+}
+int hvm64_server_poll(hvm64_server* sv, uint64_t* tickets, size_t cap, size_t* n) {
+  if (!sv || !n || (cap && !tickets)) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  *n = sv->s.poll(tickets, cap);
+  if (*n == 0) {
+    int e = 0;
+    int rc = guarded([&] { e = sv->s.device_error(); });
+    if (rc) return rc;
+    if (e) return hvm::set_error(e, std::string("the serving reducer stopped: ") + hvm::status_name(e));
+  }
+  return HVM64_OK;
+}
+int hvm64_server_result(hvm64_server* sv, uint64_t ticket, hvm64_rewrites* rw, int* status, double* device_us,
+                        char* buf, size_t cap, size_t* len) {
+  if (!sv) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  std::string text;
+  int st = 0;
+  int rc = guarded([&] { st = sv->s.result(ticket, rw, device_us, text); });
+  if (rc) return rc;
+  if (status) *status = st;
+  if (st) return hvm::set_error(st, hvm::status_name(st));
+  return copy_out(text, buf, cap, len);
+}
+void hvm64_server_free(hvm64_server* sv) { delete sv; }
+
+}  // extern "C"

@@ -17,7 +17,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HVM64_LIB") or os.path.join(HERE, "build", "libhvm64.so")
 
-OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR = range(9)
+OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR, ERR_OUTPUT = range(10)
 PERSISTENT, PLAIN = 0, 1
 
 # Every symbol include/hvm64.h declares.
@@ -26,6 +26,7 @@ EXPORTS = (
     "hvm64_book_free", "hvm64_net_create", "hvm64_net_boot", "hvm64_net_encode", "hvm64_net_normal",
     "hvm64_net_readback", "hvm64_net_free", "hvm64_batch_create", "hvm64_batch_normal", "hvm64_batch_readback",
     "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats", "hvm64_net_normal_noalloc",
+    "hvm64_server_create", "hvm64_server_submit", "hvm64_server_poll", "hvm64_server_result", "hvm64_server_free",
 )
 
 
@@ -109,6 +110,12 @@ def lib(build_if_missing=True):
     L.hvm64_net_stats.argtypes = [P, c.POINTER(Stats)]
     L.hvm64_net_normal_noalloc.argtypes = [P, c.c_char_p, c.POINTER(Tuning), c.POINTER(Rewrites), c.c_char_p,
                                            c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_server_create.argtypes = [P, c.c_uint64, c.c_uint32, c.c_uint32, c.POINTER(Tuning), c.POINTER(P)]
+    L.hvm64_server_submit.argtypes = [P, c.c_char_p, c.POINTER(c.c_uint64)]
+    L.hvm64_server_poll.argtypes = [P, c.POINTER(c.c_uint64), c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_server_result.argtypes = [P, c.c_uint64, c.POINTER(Rewrites), c.POINTER(c.c_int),
+                                      c.POINTER(c.c_double), c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_server_free.argtypes = [P]
     _lib = L
     return L
 
@@ -224,6 +231,52 @@ class Batch:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.hvm64_batch_free(self._h)
             self._h = None
+
+
+class Server:
+    """A reducer that stays on the device and admits requests while it runs.
+    `submit(name)` boots Def `name` and returns a ticket; `poll()` lists
+    finished tickets; `result(ticket)` returns (text, Rewrites, device_us).
+    While it runs, no other entry point may be used on the same device."""
+
+    def __init__(self, book, slots=256, out_pairs=1 << 16, heap_bytes=0, tuning=None):
+        self.book = book
+        self.slots = slots
+        h = ctypes.c_void_p()
+        t = ctypes.byref(tuning) if tuning is not None else None
+        _check(lib().hvm64_server_create(book._h, heap_bytes, slots, out_pairs, t, ctypes.byref(h)))
+        self._h = h
+        self._buf = (ctypes.c_uint64 * slots)()
+
+    def submit(self, name):
+        t = ctypes.c_uint64()
+        _check(lib().hvm64_server_submit(self._h, name.encode(), ctypes.byref(t)))
+        return t.value
+
+    def poll(self):
+        n = ctypes.c_size_t()
+        _check(lib().hvm64_server_poll(self._h, self._buf, self.slots, ctypes.byref(n)))
+        return [self._buf[i] for i in range(n.value)]
+
+    def result(self, ticket, cap=1 << 22):
+        rw = Rewrites()
+        st = ctypes.c_int()
+        us = ctypes.c_double()
+        n = ctypes.c_size_t()
+        buf = ctypes.create_string_buffer(cap)
+        _check(lib().hvm64_server_result(self._h, ticket, ctypes.byref(rw), ctypes.byref(st), ctypes.byref(us), buf,
+                                         cap, ctypes.byref(n)))
+        if n.value >= cap:
+            raise HvmError(ERR_BAD_INPUT, f"normal form needs {n.value + 1} bytes; pass a larger cap")
+        return buf.value.decode(), rw, us.value
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.hvm64_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def normal_noalloc(book, entry="main", tuning=None, cap=1 << 20):

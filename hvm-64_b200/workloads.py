@@ -224,3 +224,49 @@ def est_interactions(kind, depth):
     if kind == "sum":
         return 54 * (1 << depth)
     return (1 << depth) * depth * depth * (19.8 + 26.0 / depth)
+
+
+def serving_requests(n, seed=0, lo=1e3, hi=1e8):
+    """The serving stream's requests: (kind, param, j) with a target size drawn
+    log-uniform in [lo, hi] interactions; kind tree-sum / bitonic sort /
+    Church (45/45/10).  param is the depth (sum, sort) or (k, last) (Church)."""
+    rng = random.Random(splitmix64(BASE_SEED ^ (0x5E4E + seed)))
+    out = []
+    for j in range(n):
+        size = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        r = rng.random()
+        if r < 0.45:
+            d = max(3, min(20, int(round(math.log2(size / 54)))))
+            out.append(("sum", d, j))
+        elif r < 0.9:
+            d = 2
+            while d < 13 and est_interactions("sort", d) < size:
+                d += 1
+            out.append(("sort", d, j))
+        else:
+            out.append(("church", (4 if size < 1e5 else 5, 2 + j % 4), j))
+    return out
+
+
+def serving_book(reqs):
+    """One Book for a serving stream: the families' shared defs, per-request
+    generators, and request j's entry point `main_j`."""
+    parts = list(_family_defs().values())
+    for kind, param, j in reqs:
+        if kind == "church":
+            k, last = param
+            src = church(k, last)
+            for i in range(k, 0, -1):
+                src = src.replace(f"@n{i} ", f"@c{j}_n{i} ").replace(f"@n{i}\n", f"@c{j}_n{i}\n")
+            src = src.replace("@F ", f"@c{j}_F ").replace("(@F ", f"(@c{j}_F ").replace("@main ", f"@main_{j} ")
+            parts.append(src.strip())
+        else:
+            parts.append(_net_defs(kind, param, j))
+    return "\n".join(parts) + "\n"
+
+
+def check_request(kind, param, j, text):
+    """True when a served request's normal form is its expected answer."""
+    if kind == "church":
+        return text == "(* (a a))"
+    return check_result(kind, param, j, text)

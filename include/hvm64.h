@@ -36,6 +36,7 @@ extern "C" {
 #define HVM64_ERR_CUDA 6      /* CUDA runtime error (no device, launch failure) */
 #define HVM64_ERR_QUEUE 7     /* the device redex queue overflowed */
 #define HVM64_ERR_BAD_ADDR 8  /* a heap address outside the arena (internal fault, caught) */
+#define HVM64_ERR_OUTPUT 9    /* a served net's normal form did not fit its output buffer */
 
 /* Per-rule interaction counters: runtime/src/runtime.rs:72-79 (Rewrites). */
 typedef struct hvm64_rewrites {
@@ -117,6 +118,35 @@ typedef struct hvm64_stats {
 } hvm64_stats;
 int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
 int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
+
+/* Serving: one reducer that stays on the device and admits requests while it
+ * runs (continuous batching).  No reference counterpart: the reference reduces
+ * one net per call (src/main.rs:176-193, runtime/src/net.rs:55-60).
+ *
+ * hvm64_server_create uploads the Book, allocates the heap (heap_bytes, 0 =
+ * default) and `slots` net slots with an output buffer of `out_pairs`
+ * (address, word) pairs each, and launches the persistent reducer on a stream
+ * of its own.  hvm64_server_submit boots Def `def_name` in a free slot and
+ * returns a ticket (HVM64_ERR_QUEUE when every slot is taken).
+ * hvm64_server_poll writes up to `cap` finished tickets; hvm64_server_result
+ * gives a finished request's Rewrites, status, device latency (admission to
+ * completion, microseconds) and normal form (hvm64_net_readback's text
+ * convention) and frees its slot.  hvm64_server_free stops the reducer once
+ * every submitted request is done.
+ *
+ * While a server runs on a device, use no other entry point on that device
+ * (they share the reducer's launch parameters).  An error in any request
+ * (OOM, DIV0, BAD_PAIR, ...) stops the whole server; poll then returns it.
+ * A server lives at most tuning->timeout_ms (default 10 minutes), then stops
+ * with HVM64_ERR_TIMEOUT. */
+typedef struct hvm64_server hvm64_server;
+int hvm64_server_create(const hvm64_book* book, uint64_t heap_bytes, uint32_t slots, uint32_t out_pairs,
+                        const hvm64_tuning* tuning, hvm64_server** out);
+int hvm64_server_submit(hvm64_server* server, const char* def_name, uint64_t* ticket);
+int hvm64_server_poll(hvm64_server* server, uint64_t* tickets, size_t cap, size_t* n);
+int hvm64_server_result(hvm64_server* server, uint64_t ticket, hvm64_rewrites* out, int* status,
+                        double* device_us, char* buf, size_t cap, size_t* len);
+void hvm64_server_free(hvm64_server* server);
 
 /* Boot Def `def_name`, reduce it to normal form and read it back, without
  * allocating any device memory.  No counterpart in the reference.

@@ -1,0 +1,94 @@
+"""The serving reducer (hvm64_server_*): requests admitted while others are
+on the device give the same normal forms and counts as each request reduced
+alone.  GPU tests."""
+import time
+
+import pytest
+
+import workloads as W
+
+
+def _hvm():
+    import hvm64
+    return hvm64
+
+
+def _alone(hvm64, book, names):
+    """Each request reduced by itself through the one-net entry points."""
+    net = hvm64.Net(book, 2 << 30)
+    out = {}
+    for name in names:
+        net.boot(name)
+        rw = net.normal(hvm64.Tuning(timeout_ms=60000))
+        out[name] = (net.readback(), rw.as_dict())
+    del net
+    return out
+
+
+def _drain(sv, want, done, deadline):
+    while len(done) < want and time.time() < deadline:
+        for t in sv.poll():
+            done[t] = sv.result(t)
+        time.sleep(0.001)
+
+
+@pytest.mark.gpu
+def test_server_mix_matches_alone():
+    hvm64 = _hvm()
+    reqs = W.serving_requests(48, seed=7, hi=3e6)
+    book = hvm64.Book.from_str(W.serving_book(reqs))
+    names = [f"main_{j}" for _, _, j in reqs]
+    alone = _alone(hvm64, book, names)
+    for (kind, param, j), name in zip(reqs, names):
+        assert W.check_request(kind, param, j, alone[name][0]), name
+
+    sv = hvm64.Server(book, slots=64, out_pairs=1 << 16, heap_bytes=4 << 30, tuning=hvm64.Tuning(timeout_ms=120000))
+    try:
+        tickets = {}
+        done = {}
+        # the first half goes in at once; the rest arrives while it runs
+        for name in names[:24]:
+            tickets[sv.submit(name)] = name
+        for name in names[24:]:
+            time.sleep(0.0005)
+            for t in sv.poll():
+                done[t] = sv.result(t)
+            tickets[sv.submit(name)] = name
+        _drain(sv, len(names), done, time.time() + 60)
+    finally:
+        sv.close()
+    assert len(done) == len(names)
+    for t, (text, rw, us) in done.items():
+        name = tickets[t]
+        assert text == alone[name][0], name
+        assert rw.as_dict() == alone[name][1], name
+        assert us > 0
+
+
+@pytest.mark.gpu
+def test_server_slots_and_reuse():
+    """A full server refuses a request (HVM64_ERR_QUEUE); slots freed by
+    collected results take new requests, many times over."""
+    hvm64 = _hvm()
+    reqs = [("sum", 8, j) for j in range(6)]
+    book = hvm64.Book.from_str(W.serving_book(reqs))
+    sv = hvm64.Server(book, slots=4, out_pairs=1 << 10, heap_bytes=1 << 30, tuning=hvm64.Tuning(timeout_ms=120000))
+    try:
+        owner = {sv.submit(f"main_{j}"): j for j in range(4)}
+        with pytest.raises(hvm64.HvmError) as e:
+            sv.submit("main_4")
+        assert e.value.code == hvm64.ERR_QUEUE
+        for round_ in range(10):
+            got = {}
+            _drain(sv, 4, got, time.time() + 20)
+            assert len(got) == 4
+            for t, (text, rw, us) in got.items():
+                assert text == str(W.expected_sum(8, owner.pop(t)))
+            for k in range(4):
+                j = (round_ + k) % 6
+                owner[sv.submit(f"main_{j}")] = j
+        got = {}
+        _drain(sv, 4, got, time.time() + 20)
+        assert len(got) == 4
+    finally:
+        sv.close()
