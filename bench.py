@@ -279,6 +279,8 @@ def main():
     ap.add_argument("--device-only", action="store_true", help="skip the plain, e2e, serving and CPU legs")
     ap.add_argument("--serve-requests", type=int, default=96, help="requests per offered load (0: no serving leg)")
     ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--autotune", type=int, default=1, help="pick the launch knobs on a sample first (0: defaults)")
+    ap.add_argument("--tune-sample", type=int, default=256)
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -302,8 +304,14 @@ def main():
     book = hvm64.Book.from_str(text)
     names = [f"main_{j}" for _, _, j in entries]
     heap = int(args.heap_gb * (1 << 30))
+    tune_report = None
+    if args.autotune:
+        import autotune
+        tune, tune_report = autotune.autotune(book, names, heap, sample=args.tune_sample, timeout_ms=600000)
+    else:
+        tune = hvm64.Tuning(timeout_ms=600000)
+    tune.flags |= hvm64.TUNE_GRAPH  # each step replays one captured CUDA graph
     batch = hvm64.Batch(book, names, heap)
-    tune = hvm64.Tuning(timeout_ms=600000)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
@@ -360,6 +368,9 @@ def main():
                      "kernel": "reduce_kernel (+ boot_kernel) device time per launch", "kernel_ms": kms,
                      "algorithmic_bytes": alg},
         "gpu_launches": 4 * args.steps,
+        "tuning": {"knobs": {k: getattr(tune, k) for k in ("blocks_per_sm", "chunk_nodes", "donate_min",
+                                                            "queue_slots_log2")},
+                   "cuda_graph": True, "autotune": tune_report},
         "clocks": clk.summary(),
         "device_stats": stats,
     }
@@ -369,11 +380,12 @@ def main():
         plain_entries = entries[:args.plain_nets]
         if plain_entries:
             pbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
-            pbatch.normal(hvm64.PLAIN, tune)
+            ptune = hvm64.Tuning(timeout_ms=600000)
+            pbatch.normal(hvm64.PLAIN, ptune)
             ptotal = sum(pbatch.rwts[i].total() for i in range(pbatch.n))
             torch.cuda.synchronize()
             p0 = time.perf_counter()
-            pbatch.normal(hvm64.PLAIN, tune)
+            pbatch.normal(hvm64.PLAIN, ptune)
             plain_s = time.perf_counter() - p0
             pdev = pbatch.device_ms
             del pbatch

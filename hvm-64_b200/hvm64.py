@@ -19,6 +19,7 @@ LIB_PATH = os.environ.get("HVM64_LIB") or os.path.join(HERE, "build", "libhvm64.
 
 OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR, ERR_OUTPUT = range(10)
 PERSISTENT, PLAIN = 0, 1
+TUNE_GRAPH = 1  # Tuning.flags: persistent runs replay one captured CUDA graph
 
 # Every symbol include/hvm64.h declares.
 EXPORTS = (
@@ -60,7 +61,7 @@ class Rewrites(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("chunk_nodes", ctypes.c_uint32),
                 ("donate_min", ctypes.c_uint32), ("queue_slots_log2", ctypes.c_uint32),
-                ("lane_budget", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("lane_budget", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("timeout_ms", ctypes.c_uint64)]
 
 

@@ -50,9 +50,14 @@ typedef struct hvm64_tuning {
   uint32_t donate_min;       /* warp-stack depth above which a warp shares work */
   uint32_t queue_slots_log2; /* global redex-queue capacity, in 32-redex slots */
   uint32_t lane_budget;      /* interactions a lane may do per warp step */
-  uint32_t reserved;         /* must be 0 */
+  uint32_t flags;            /* HVM64_TUNE_* bits */
   uint64_t timeout_ms;       /* run deadline; a longer run fails with TIMEOUT */
 } hvm64_tuning;
+
+/* A persistent batch run is captured once as a CUDA graph (uploads, queue
+ * init, boot and reducer launches) and replayed by later runs of the same
+ * batch and tuning. */
+#define HVM64_TUNE_GRAPH 1u
 
 typedef struct hvm64_book hvm64_book;
 typedef struct hvm64_net hvm64_net;

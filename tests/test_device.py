@@ -81,6 +81,24 @@ def test_plain_equals_persistent_and_repeats():
 
 
 @pytest.mark.gpu
+def test_graph_replay_equals_direct_launch():
+    """A persistent batch captured as a CUDA graph and replayed gives the
+    same forms and counts as the direct launches, on every replay."""
+    import workloads as W
+    hvm64 = _hvm()
+    entries = W.batch_entries(16, 4, 9, seed=13)
+    book = hvm64.Book.from_str(W.batch_book(entries))
+    names = [f"main_{j}" for _, _, j in entries]
+    b = hvm64.Batch(book, names, 1 << 30)
+    b.normal(hvm64.PERSISTENT, hvm64.Tuning(timeout_ms=60000))
+    want = [(b.readback(i), b.rwts[i].as_dict()) for i in range(b.n)]
+    g = hvm64.Tuning(timeout_ms=60000, flags=hvm64.TUNE_GRAPH)
+    for _ in range(3):
+        b.normal(hvm64.PERSISTENT, g)
+        assert [(b.readback(i), b.rwts[i].as_dict()) for i in range(b.n)] == want
+
+
+@pytest.mark.gpu
 def test_batch_expression_and_trivial_entries():
     """Entries may be expression nets ('=' prefix), nets with no redex at
     all, and Def boots, mixed in one batch."""
