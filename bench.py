@@ -9,8 +9,10 @@ reference's Rewrites::total) per second, in G/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank reduces its own batch (seeded by rank): weak scaling,
-no collective on the data path (the nets are independent).
+Under torchrun the job reduces nets x N nets, split over the ranks by a
+size-balanced partition (weak scaling: each GPU keeps about `nets` nets); no
+collective on the data path (the nets are independent), only the step time
+(max over ranks) and the interaction count (sum) are reduced.
 `--impl reference` times the CPU evaluator (the oracle's restatement of the
 reference's Net::parallel_normal; the Rust reference cannot be built without
 a Rust toolchain) on a bounded sample of the same workload.
@@ -238,7 +240,7 @@ def config(args):
                         f"[{args.dmin}, {args.dmax}], u24 keys",
             "nets": args.nets, "dmin": args.dmin, "dmax": args.dmax, "mode": "persistent, one launch per step",
             "l2": "flushed between steps (512 MiB write); heaps far above L2",
-            "parallelism": f"weak: {args.gpus} x 1 GPU, disjoint nets per rank"}
+            "parallelism": f"weak: {args.gpus} x 1 GPU, size-balanced disjoint shares of nets x {args.gpus} nets"}
 
 
 def run_reference(args):
@@ -299,7 +301,14 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     import hvm64
-    entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=rank)
+    if world > 1:
+        # one global batch of nets x world nets, split into size-balanced
+        # shares (no communication while they reduce)
+        import shard
+        glob = W.batch_entries(args.nets * world, args.dmin, args.dmax, seed=0)
+        entries = shard.rank_share(glob, lambda e: W.est_interactions(e[0], e[1]), rank, world)
+    else:
+        entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=0)
     text = W.batch_book(entries)
     book = hvm64.Book.from_str(text)
     names = [f"main_{j}" for _, _, j in entries]
