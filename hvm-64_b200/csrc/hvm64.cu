@@ -161,12 +161,15 @@ __device__ void flush_counters(WarpSmem& W, int cur) {
 // through.  Lane 0 walks it depth-first, using the warp's redex ring (empty
 // when a net completes) as its stack, and writes the pairs into the slot's
 // output in mapped host memory.
-__device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull root, int& status) {
-  ull* out = g_P.out + ull(slot) * g_P.out_cap * 2;
-  const unsigned cap = g_P.out_cap;
+// Walks net `net`'s normal form from word `root` the way host readback does
+// (host/src/readback.rs:23-87): the root word, both words of every node it
+// reaches, each redirect chain a Var goes through.  Writes the first `cap`
+// (address, word) pairs to `out` and returns how many there are; `stk` (scap
+// entries) is the depth-first stack.  *deep is set when the stack overflowed
+// (the count is then incomplete).
+__device__ __noinline__ unsigned gather_walk(unsigned net, ull root, ull* out, unsigned cap, ull* stk,
+                                             unsigned scap, bool* deep) {
   const ull hb = g_P.heap_bytes;
-  ull* stk = W.stk;
-  const unsigned scap = 2 * SCAP;
   unsigned sp = 0, n = 0;
   auto emit = [&](ull w, ull v) {
     if (n < cap) {
@@ -182,14 +185,14 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
   stk[sp++] = root;
   while (sp) {
     ull w = stk[--sp];
-    ull v = ld_gpu(heap_at(slot, w));
+    ull v = ld_gpu(heap_at(net, w));
     emit(w, v);
     unsigned t = unsigned(v & 7);
     if (t == T_VAR || t == T_RED) {
       if (live(v)) {
         ull e = paddr(v);
         for (unsigned g = 0; g < (1u << 20); g++) {
-          ull x = ld_gpu(heap_at(slot, e));
+          ull x = ld_gpu(heap_at(net, e));
           emit(e, x);
           if ((x & 7) != T_RED || !live(x)) break;
           e = paddr(x);
@@ -197,19 +200,44 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
       }
     } else if (t == T_OP || t == T_CTR || t == T_SWITCH) {
       if (sp + 2 > scap) {
-        status = HVM64_ERR_OUTPUT;
+        *deep = true;
         break;
       }
       ull a = paddr(v);
       stk[sp++] = a ^ 8;
       stk[sp++] = a;
     }
-    if (n > cap) {
-      status = HVM64_ERR_OUTPUT;
-      break;
-    }
   }
-  return n < cap ? n : cap;
+  return n;
+}
+
+// A served net's normal form leaves the device as gathered pairs in the
+// slot's output (mapped host memory).  Lane 0 walks it, using the warp's redex
+// ring (empty when a net completes) as its stack.
+__device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull root, int& status) {
+  ull* out = g_P.out + ull(slot) * g_P.out_cap * 2;
+  bool deep = false;
+  unsigned n = gather_walk(slot, root, out, g_P.out_cap, W.stk, 2 * SCAP, &deep);
+  if (deep || n > g_P.out_cap) status = HVM64_ERR_OUTPUT;
+  return n < g_P.out_cap ? n : g_P.out_cap;
+}
+
+// Batch readback on the device: one thread per net counts (out == nullptr)
+// or writes its net's pairs at offs[i].  A net whose walk overflows the
+// stack gets count ~0u and is read back from a heap image instead.
+constexpr unsigned GATHER_STACK = 256;
+__global__ void gather_kernel(unsigned n, unsigned* counts, const ull* offs, ull* out) {
+  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ull stk[GATHER_STACK];
+  bool deep = false;
+  ull root = g_P.nets[i].root;
+  if (!out) {
+    unsigned c = gather_walk(i, root, nullptr, 0, stk, GATHER_STACK, &deep);
+    counts[i] = deep ? ~0u : c;
+  } else if (counts[i] != ~0u) {
+    gather_walk(i, root, out + 2 * offs[i], counts[i], stk, GATHER_STACK, &deep);
+  }
 }
 
 // The net in `slot` reached normal form: gather it and post its completion
@@ -499,7 +527,13 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
     }
     // A step of Def calls: stage that Def's instructions in shared memory
     // (one cooperative load instead of a dependent fetch per instruction).
-    if (key >= 64u && key - 64u < g_P.ndefs && key - 64u != W.icache_def) {
+    // Every lane reads the staged Def's index before lane 0 may replace it:
+    // lanes are not guaranteed to run this in lock-step, and a lane that saw
+    // the new index would skip its share of the copy.
+    __syncwarp();
+    const unsigned staged = W.icache_def;
+    __syncwarp();
+    if (key >= 64u && key - 64u < g_P.ndefs && key - 64u != staged) {
       unsigned id = key - 64u;
       const DevDef d = g_P.defs[id];
       if (d.ins_len <= ICACHE) {
@@ -902,6 +936,7 @@ struct Runner {
     }
     if (device_ms) *device_ms = total_ms;
     image_valid = false;
+    pairs_valid = false;
     reduced = true;
   }
 
@@ -1033,9 +1068,53 @@ struct Runner {
     o->idle_cycles = stat_idle;
   }
 
+  // Normal forms gathered on the device (gather_kernel): per net, its
+  // (address, word) pairs; a count of ~0u sends that net to the heap image.
+  bool pairs_valid = false;
+  std::vector<unsigned> gcount;
+  std::vector<uint64_t> goff, gpairs;
+  DevBuf<unsigned> d_gcount;
+  DevBuf<dev::ull> d_goff, d_gpairs;
+
+  void gather_all() {
+    unsigned n = unsigned(progs.size());
+    dev::Params p = params();
+    CU(cudaMemcpyToSymbol(dev::g_P, &p, sizeof p));
+    d_gcount.alloc(n);
+    unsigned blocks = (n + 127) / 128;
+    dev::gather_kernel<<<blocks, 128>>>(n, d_gcount.p, nullptr, nullptr);
+    CU(cudaGetLastError());
+    gcount.resize(n);
+    CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    goff.resize(n);
+    uint64_t tot = 0;
+    for (unsigned i = 0; i < n; i++) {
+      goff[i] = tot;
+      if (gcount[i] != ~0u) tot += gcount[i];
+    }
+    d_goff.alloc(n);
+    CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
+    d_gpairs.alloc(2 * tot);
+    dev::gather_kernel<<<blocks, 128>>>(n, d_gcount.p, d_goff.p, d_gpairs.p);
+    CU(cudaGetLastError());
+    gpairs.resize(2 * tot);
+    if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
+    d2h += size_t(n) * 4 + 16 * tot;
+    h2d += size_t(n) * 8;
+    pairs_valid = true;
+  }
+
   std::string readback(unsigned i) {
     if (!reduced) throw Error(HVM64_ERR_BAD_INPUT, "net not reduced yet");
     if (host_nets[i].status) throw Error(host_nets[i].status, status_name(host_nets[i].status));
+    if (!pairs_valid) gather_all();
+    if (gcount[i] != ~0u) {
+      std::string out;
+      with_big_stack([&] {
+        out = hvm::readback_pairs(book, gpairs.data() + 2 * goff[i], gcount[i], heap_bytes / 8, host_nets[i].root);
+      });
+      return out;
+    }
     if (!image_valid) {
       // Copy the used part of the heap (everything below the bump pointer).
       uint64_t used = 0;

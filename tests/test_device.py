@@ -132,6 +132,25 @@ def test_tree_sum_depth18_full_size():
 
 
 @pytest.mark.gpu
+def test_repeated_runs_identical():
+    """The same net reduced eight times on one heap (which keeps the previous
+    run's words) gives the same normal form and counts every time: a check
+    against scheduling-dependent races, which show up as occasional wrong
+    results."""
+    import workloads as W
+    hvm64 = _hvm()
+    text = W.tree_sum(18, 0)
+    net = hvm64.Net(hvm64.Book.from_str(text), 4 << 30)
+    seen = set()
+    for _ in range(8):
+        net.boot("main")
+        rw = net.normal(hvm64.Tuning(timeout_ms=60000))
+        seen.add((net.readback(), tuple(sorted(rw.as_dict().items()))))
+    assert len(seen) == 1
+    assert next(iter(seen))[0] == str(W.expected_sum(18, 0))
+
+
+@pytest.mark.gpu
 def test_bitonic_depth15_sorted():
     """Bitonic sort of 2^15 keys: the read-back leaves are the sorted input
     multiset (size-independent check), counts equal the oracle's."""
