@@ -282,7 +282,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=96, help="requests per offered load (0: no serving leg)")
     ap.add_argument("--serve-slots", type=int, default=64)
     ap.add_argument("--autotune", type=int, default=1, help="pick the launch knobs on a sample first (0: defaults)")
-    ap.add_argument("--tune-sample", type=int, default=256)
+    ap.add_argument("--tune-sample", type=int, default=1024)
     args = ap.parse_args()
 
     if args.impl == "reference":

@@ -15,10 +15,10 @@ import hvm64
 
 # Candidate values per knob; 0 is the library default.
 SPACE = {
-    "blocks_per_sm": (0, 6, 5, 4),
-    "chunk_nodes": (0, 64, 1024, 4096),
-    "donate_min": (0, 32, 128, 256),
-    "queue_slots_log2": (0, 14, 18),
+    "blocks_per_sm": (0, 6, 4),
+    "chunk_nodes": (0, 4096),
+    "donate_min": (0, 32, 128),
+    "queue_slots_log2": (0, 18),
 }
 ORDER = ("blocks_per_sm", "chunk_nodes", "donate_min", "queue_slots_log2")
 

@@ -677,14 +677,22 @@ struct Reader {
   std::unordered_map<uint64_t, size_t> vars;
   size_t next_var = 0;
   std::string o;
-  const std::unordered_map<uint64_t, uint64_t>* sparse = nullptr;  // gathered words, by address
+  // Gathered (address, word) pairs.  The device walk visits words in the
+  // order this reader loads them, so a cursor serves almost every load; the
+  // address map is built only if a load ever misses it.
+  const uint64_t* pairs = nullptr;
+  size_t npairs = 0, cursor = 0;
+  std::unordered_map<uint64_t, uint64_t> sparse;
 
-  uint64_t load(uint64_t addr) const {
+  uint64_t load(uint64_t addr) {
     uint64_t w = addr >> 3;
     if (w >= words) throw Error(HVM64_ERR_BAD_INPUT, "readback: address outside the heap");
-    if (sparse) {
-      auto it = sparse->find(addr);
-      if (it == sparse->end()) throw Error(HVM64_ERR_BAD_INPUT, "readback: word not gathered");
+    if (pairs) {
+      if (cursor < npairs && pairs[2 * cursor] == addr) return pairs[2 * cursor++ + 1];
+      if (sparse.empty())
+        for (size_t i = 0; i < npairs; i++) sparse[pairs[2 * i]] = pairs[2 * i + 1];
+      auto it = sparse.find(addr);
+      if (it == sparse.end()) throw Error(HVM64_ERR_BAD_INPUT, "readback: word not gathered");
       return it->second;
     }
     return heap[w];
@@ -771,11 +779,9 @@ std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words
 
 std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npairs, uint64_t heap_words,
                            uint64_t root) {
-  std::unordered_map<uint64_t, uint64_t> m;
-  m.reserve(npairs * 2);
-  for (size_t i = 0; i < npairs; i++) m[pairs[2 * i]] = pairs[2 * i + 1];
   Reader r{book, nullptr, heap_words, {}, 0, {}};
-  r.sparse = &m;
+  r.pairs = pairs;
+  r.npairs = npairs;
   r.wire(root);
   return r.o;
 }

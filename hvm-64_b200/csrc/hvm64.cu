@@ -310,6 +310,11 @@ __device__ __noinline__ unsigned serve_admit(WarpSmem& W, Ctx& c) {
   return slot + 1;
 }
 
+#ifndef HVM_QW
+#define HVM_QW 2
+#endif
+constexpr int QW = HVM_QW;  // selection window: 32 * QW newest redexes
+
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
@@ -468,58 +473,61 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       if (lane == 0) atomicAdd(&C->stat_spilled, 1ull);
     }
 
-    // Choose this step's redexes: among the newest 64, the rule class most
-    // common among the newest 32 (ties: the newest); up to 32 of that class
-    // run this step, one per lane, and the others go back on the stack.
-    unsigned w = min(top - bot, 64u);
-    ull a0 = 0, b0 = 0, a1 = 0, b1 = 0;
-    bool h0 = lane < w, h1 = lane + 32 < w;
-    if (h0) {
-      unsigned k = (top - 1 - lane) & (SCAP - 1);
-      a0 = S[2 * k];
-      b0 = S[2 * k + 1];
+    // Choose this step's redexes: among the newest 32 * QW, the rule class
+    // most common among the newest 32 (ties: the newest); up to 32 of that
+    // class run this step, one per lane, and the others go back on the stack
+    // in their order.
+    const unsigned w = min(top - bot, unsigned(32 * QW));
+    ull qa[QW], qb[QW];
+    bool qh[QW];
+    unsigned qk[QW];
+#pragma unroll
+    for (int q = 0; q < QW; q++) {
+      qh[q] = lane + 32u * q < w;
+      qa[q] = qb[q] = 0;
+      if (qh[q]) {
+        unsigned k = (top - 1 - 32u * q - lane) & (SCAP - 1);
+        qa[q] = S[2 * k];
+        qb[q] = S[2 * k + 1];
+      }
+      qk[q] = qh[q] ? redex_class(qa[q], qb[q]) : 0xFFFFFFF0u + unsigned(q);
     }
-    if (h1) {
-      unsigned k = (top - 33 - lane) & (SCAP - 1);
-      a1 = S[2 * k];
-      b1 = S[2 * k + 1];
-    }
-    unsigned k0 = h0 ? redex_class(a0, b0) : 0xFFFFFFFFu;
-    unsigned k1 = h1 ? redex_class(a1, b1) : 0xFFFFFFFEu;
-    unsigned peers = __match_any_sync(0xffffffffu, k0);
-    unsigned score = h0 ? ((unsigned(__popc(peers)) << 8) | (255u - lane)) : 0u;
+    unsigned peers = __match_any_sync(0xffffffffu, qk[0]);
+    unsigned score = qh[0] ? ((unsigned(__popc(peers)) << 8) | (255u - lane)) : 0u;
     unsigned best = __reduce_max_sync(0xffffffffu, score);
-    unsigned key = __shfl_sync(0xffffffffu, k0, int(255u - (best & 255u)));
-    bool s0 = h0 && k0 == key, s1 = h1 && k1 == key;
-    unsigned m0 = __ballot_sync(0xffffffffu, s0), m1 = __ballot_sync(0xffffffffu, s1);
-    unsigned n0 = unsigned(__popc(m0));
-    unsigned r0 = unsigned(__popc(m0 & lt)), r1 = n0 + unsigned(__popc(m1 & lt));
-    bool t1 = s1 && r1 < 32u;
-    bool u0 = h0 && !s0, u1 = h1 && !t1;
-    unsigned um0 = __ballot_sync(0xffffffffu, u0), um1 = __ballot_sync(0xffffffffu, u1);
-    unsigned n = min(n0 + unsigned(__popc(m1)), 32u);
+    unsigned key = __shfl_sync(0xffffffffu, qk[0], int(255u - (best & 255u)));
+    unsigned nsel = 0, sr[QW], um[QW];
+    bool st[QW], su[QW];
+#pragma unroll
+    for (int q = 0; q < QW; q++) {
+      bool sq = qh[q] && qk[q] == key;
+      unsigned m = __ballot_sync(0xffffffffu, sq);
+      sr[q] = nsel + unsigned(__popc(m & lt));
+      st[q] = sq && sr[q] < 32u;
+      nsel += unsigned(__popc(m));
+      su[q] = qh[q] && !st[q];
+      um[q] = __ballot_sync(0xffffffffu, su[q]);
+    }
+    unsigned n = min(nsel, 32u);
     unsigned base = top - w;
     __syncwarp();
-    if (s0) {
-      W.sel[2 * r0] = a0;
-      W.sel[2 * r0 + 1] = b0;
+    // Entries that stay keep their relative depth (older quarters lower; in a
+    // quarter, higher lanes are older).
+    unsigned below = 0;
+#pragma unroll
+    for (int q = QW - 1; q >= 0; q--) {
+      if (st[q]) {
+        W.sel[2 * sr[q]] = qa[q];
+        W.sel[2 * sr[q] + 1] = qb[q];
+      }
+      if (su[q]) {
+        unsigned k = (base + below + unsigned(__popc(um[q] & gt))) & (SCAP - 1);
+        S[2 * k] = qa[q];
+        S[2 * k + 1] = qb[q];
+      }
+      below += unsigned(__popc(um[q]));
     }
-    if (t1) {
-      W.sel[2 * r1] = a1;
-      W.sel[2 * r1 + 1] = b1;
-    }
-    // Entries that stay keep their relative depth (deeper ones lower).
-    if (u1) {
-      unsigned k = (base + unsigned(__popc(um1 & gt))) & (SCAP - 1);
-      S[2 * k] = a1;
-      S[2 * k + 1] = b1;
-    }
-    if (u0) {
-      unsigned k = (base + unsigned(__popc(um1)) + unsigned(__popc(um0 & gt))) & (SCAP - 1);
-      S[2 * k] = a0;
-      S[2 * k + 1] = b0;
-    }
-    top = base + unsigned(__popc(um0)) + unsigned(__popc(um1));
+    top = base + below;
     if (lane == 0) {
       W.ring_cnt = 0;
       W.ring_base = top;
