@@ -161,56 +161,6 @@ __device__ void flush_counters(WarpSmem& W, int cur) {
 // through.  Lane 0 walks it depth-first, using the warp's redex ring (empty
 // when a net completes) as its stack, and writes the pairs into the slot's
 // output in mapped host memory.
-// Walks net `net`'s normal form from word `root` the way host readback does
-// (host/src/readback.rs:23-87): the root word, both words of every node it
-// reaches, each redirect chain a Var goes through.  Writes the first `cap`
-// (address, word) pairs to `out` and returns how many there are; `stk` (scap
-// entries) is the depth-first stack.  *deep is set when the stack overflowed
-// (the count is then incomplete).
-__device__ __noinline__ unsigned gather_walk(unsigned net, ull root, ull* out, unsigned cap, ull* stk,
-                                             unsigned scap, bool* deep) {
-  const ull hb = g_P.heap_bytes;
-  unsigned sp = 0, n = 0;
-  auto emit = [&](ull w, ull v) {
-    if (n < cap) {
-      out[2 * n] = w;
-      out[2 * n + 1] = v;
-    }
-    n++;
-  };
-  auto live = [&](ull p) {
-    ull a = p & A_MASK;
-    return (p >> 48) == 0 && a != 0 && a < hb;
-  };
-  stk[sp++] = root;
-  while (sp) {
-    ull w = stk[--sp];
-    ull v = ld_gpu(heap_at(net, w));
-    emit(w, v);
-    unsigned t = unsigned(v & 7);
-    if (t == T_VAR || t == T_RED) {
-      if (live(v)) {
-        ull e = paddr(v);
-        for (unsigned g = 0; g < (1u << 20); g++) {
-          ull x = ld_gpu(heap_at(net, e));
-          emit(e, x);
-          if ((x & 7) != T_RED || !live(x)) break;
-          e = paddr(x);
-        }
-      }
-    } else if (t == T_OP || t == T_CTR || t == T_SWITCH) {
-      if (sp + 2 > scap) {
-        *deep = true;
-        break;
-      }
-      ull a = paddr(v);
-      stk[sp++] = a ^ 8;
-      stk[sp++] = a;
-    }
-  }
-  return n;
-}
-
 // A served net's normal form leaves the device as gathered pairs in the
 // slot's output (mapped host memory).  Lane 0 walks it, using the warp's redex
 // ring (empty when a net completes) as its stack.

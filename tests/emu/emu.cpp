@@ -198,6 +198,23 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     for (int k = 0; k < 5; k++) rw[k] = E.nets[0].rw[k];
     std::string txt;
     with_big_stack([&] { txt = readback(book, reinterpret_cast<const uint64_t*>(E.heap.data()), E.heap.size(), E.nets[0].root); });
+    // The device-side gather (the words readback loads, in its order) must
+    // read back to the same text.
+    {
+      std::vector<ull> pairs(2 * 4096), stk(256);
+      bool deep = false;
+      unsigned n = gather_walk(0, E.nets[0].root, pairs.data(), 4096, stk.data(), 256, &deep);
+      if (!deep && n > 4096) {
+        pairs.assign(2 * size_t(n), 0);
+        n = gather_walk(0, E.nets[0].root, pairs.data(), n, stk.data(), 256, &deep);
+      }
+      if (!deep) {
+        std::string g;
+        with_big_stack([&] { g = readback_pairs(book, reinterpret_cast<const uint64_t*>(pairs.data()), n,
+                                                E.heap.size(), E.nets[0].root); });
+        if (g != txt) throw Error(HVM64_ERR_BAD_INPUT, "gathered readback differs: " + g.substr(0, 80));
+      }
+    }
     *out_text = strdup(txt.c_str());
     return 0;
   } catch (Error& e) {
