@@ -470,6 +470,23 @@ struct Encoder {
   std::vector<RawInstr> out;
   uint32_t trgs = 1;
   std::map<std::string, uint32_t> scope;
+  // Emit the smaller child of a binary node first.  A child's wire stays live
+  // while its sibling's subtree is emitted, so a deeply one-sided literal tree
+  // needs one live wire per level in the reference's order (first child
+  // first) and a constant number this way.  Used only for Defs that would not
+  // fit the device register file otherwise.
+  bool small_first = false;
+  std::unordered_map<const Tree*, size_t> sizes;
+
+  size_t size(const Tree* t) {
+    if (!t) return 0;
+    auto it = sizes.find(t);
+    if (it != sizes.end()) return it->second;
+    size_t n = 1 + size(t->p1) + size(t->p2);
+    sizes[t] = n;
+    return n;
+  }
+  bool swap_children(const Tree* a, const Tree* b) { return small_first && size(b) < size(a); }
 
   uint32_t fresh() { return trgs++; }
   uint64_t ref(const std::string& n) {
@@ -515,8 +532,13 @@ struct Encoder {
       case K_CTR: {
         uint32_t p1 = fresh(), p2 = fresh();
         out.push_back({I_CTR, 0, t->lab, trg, p1, p2, 0, 0});
-        tree(t->p1, p1);
-        tree(t->p2, p2);
+        if (swap_children(t->p1, t->p2)) {
+          tree(t->p2, p2);
+          tree(t->p1, p1);
+        } else {
+          tree(t->p1, p1);
+          tree(t->p2, p2);
+        }
         return;
       }
       case K_OP: {
@@ -535,16 +557,26 @@ struct Encoder {
         } else {
           uint32_t r = fresh(), out_t = fresh();
           out.push_back({I_OP, op, 0, trg, r, out_t, 0, 0});
-          tree(rhs, r);
-          tree(o, out_t);
+          if (swap_children(rhs, o)) {
+            tree(o, out_t);
+            tree(rhs, r);
+          } else {
+            tree(rhs, r);
+            tree(o, out_t);
+          }
         }
         return;
       }
       case K_SWITCH: {
         uint32_t arms = fresh(), o = fresh();
         out.push_back({I_SWITCH, 0, 0, trg, arms, o, 0, 0});
-        tree(t->p1, arms);
-        tree(t->p2, o);
+        if (swap_children(t->p1, t->p2)) {
+          tree(t->p2, o);
+          tree(t->p1, arms);
+        } else {
+          tree(t->p1, arms);
+          tree(t->p2, o);
+        }
         return;
       }
       case K_VAR: {
@@ -620,6 +652,23 @@ static void emit(Book& book, const std::vector<RawInstr>& raw, uint32_t nregs, D
 }
 }  // namespace
 
+// Encodes a Def's net into device instructions: in the reference's order,
+// or smaller-child-first when that order needs more than MAX_REGS registers.
+static uint32_t encode_net(Book& book, const AstNet& net, DevDef& d) {
+  for (int pass = 0; pass < 2; pass++) {
+    Encoder e{book, {}, 1, {}};
+    e.small_first = pass == 1;
+    e.net(net, 0);
+    if (!e.scope.empty()) throw Error(HVM64_ERR_BAD_INPUT, "unbound variables: " + e.scope.begin()->first);
+    uint32_t nregs = rename(e.out, e.trgs);
+    if (nregs <= MAX_REGS || pass == 1) {
+      emit(book, e.out, nregs, d);
+      return nregs;
+    }
+  }
+  return 0;
+}
+
 void Book::load(const AstBook& b) {
   keep.push_back(b.arena);
   // Phase 1: ids and label sets (host.rs:54-65); phase 2: instructions.
@@ -637,12 +686,8 @@ void Book::load(const AstBook& b) {
   defs.resize(names.size());
   for (auto& [name, net] : b.nets) {
     uint32_t id = ids[name];
-    Encoder e{*this, {}, 1, {}};
-    e.net(net, 0);
-    if (!e.scope.empty()) throw Error(HVM64_ERR_BAD_INPUT, "unbound variables: " + e.scope.begin()->first);
     DevDef d{};
-    uint32_t nregs = rename(e.out, e.trgs);
-    emit(*this, e.out, nregs, d);
+    encode_net(*this, net, d);
     d.min_safe = labs[id].min_safe;
     d.lab_off = uint32_t(labbits.size());
     d.lab_len = uint32_t(labs[id].bits.size());
@@ -652,12 +697,8 @@ void Book::load(const AstBook& b) {
 }
 
 uint32_t Book::add_expr(const AstNet& net) {
-  Encoder e{*this, {}, 1, {}};
-  e.net(net, 0);
-  if (!e.scope.empty()) throw Error(HVM64_ERR_BAD_INPUT, "unbound variables: " + e.scope.begin()->first);
   DevDef d{};
-  uint32_t nregs = rename(e.out, e.trgs);
-  emit(*this, e.out, nregs, d);
+  encode_net(*this, net, d);
   d.min_safe = 0;
   d.lab_off = 0;
   d.lab_len = 0;

@@ -206,3 +206,19 @@ def test_error_status(case):
     # the device is still usable afterwards
     got, _ = hvm64.run_book("@main = x & 3 ~ $([*] $(5 x))\n", heap_bytes=1 << 24)
     assert got == "15"
+
+
+@pytest.mark.gpu
+def test_deep_normal_form_reads_back():
+    """A normal form nested deeper than the device gather's stack (a
+    left-nested tree of depth 300) is read back through the heap image
+    instead, with the same text as the oracle's."""
+    hvm64, oracle = _hvm(), _oracle()
+    t = "*"
+    for i in range(300):
+        t = f"({t} {i % 7})"
+    src = f"@deep = {t}\n@main = x & @deep ~ x\n"
+    want, want_rw, _ = oracle.run_book(src)
+    got, rw = hvm64.run_book(src, heap_bytes=1 << 28)
+    assert got == want
+    assert rw == want_rw

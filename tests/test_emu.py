@@ -54,3 +54,20 @@ def test_emu_workloads():
     assert text == str(W.expected_sum(12, 3))
     text, _ = emu_run(W.bitonic(9, 4), threads=32)
     assert W.leaves(text) == sorted(W.sort_keys(9, 4))
+
+
+def test_emu_deep_literal_def():
+    """A Def whose literal tree is 300 levels deep on one side needs more live
+    wires than the device register file in the reference's emission order;
+    the encoder emits it smaller-child-first, with the same normal form and
+    counts as the oracle's."""
+    from oracle import oracle
+    for left in (True, False):
+        t = "*"
+        for i in range(300):
+            t = f"({t} {i % 7})" if left else f"({i % 7} {t})"
+        src = f"@deep = {t}\n@main = x & @deep ~ x\n"
+        want, want_rw, _ = oracle.run_book(src)
+        text, rw = emu_run(src, threads=4)
+        assert text == want
+        assert rw == want_rw

@@ -92,3 +92,26 @@ def test_server_slots_and_reuse():
         assert len(got) == 4
     finally:
         sv.close()
+
+
+@pytest.mark.gpu
+def test_server_error_stops_it_cleanly():
+    """A request that divides by zero stops the whole server; poll reports
+    the error, close returns, and the device stays usable."""
+    hvm64 = _hvm()
+    src = "@bad = x & 10 ~ $([/] $(0 x))\n@ok = x & 3 ~ $([*] $(5 x))\n"
+    book = hvm64.Book.from_str(src)
+    sv = hvm64.Server(book, slots=4, out_pairs=1 << 10, heap_bytes=1 << 28, tuning=hvm64.Tuning(timeout_ms=60000))
+    try:
+        sv.submit("bad")
+        deadline = time.time() + 30
+        with pytest.raises(hvm64.HvmError) as e:  # from poll, or from the failed request's result
+            while time.time() < deadline:
+                for t in sv.poll():
+                    sv.result(t)
+                time.sleep(0.001)
+        assert e.value.code == hvm64.ERR_DIV0
+    finally:
+        sv.close()
+    got, _ = hvm64.run_book(src.replace("@ok", "@main"), heap_bytes=1 << 24)
+    assert got == "15"
