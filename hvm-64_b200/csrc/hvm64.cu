@@ -800,6 +800,7 @@ struct Runner {
     unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : 16;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
     h2d = d2h = 0;
+    error_detail.clear();
     heap.alloc(heap_bytes / 8);
     ctrl.alloc(1);
     nets.alloc(progs.size());
@@ -860,6 +861,7 @@ struct Runner {
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
       if (host_ctrl.error) {
         for (unsigned k = first; k < first + count; k++) host_nets[k].status = host_ctrl.error;
+        note_error(host_ctrl);
       }
     };
     if (mode == HVM64_BATCH_PLAIN) {
@@ -876,8 +878,10 @@ struct Runner {
       stat_busy += host_ctrl.stat_busy_cycles;
       stat_idle += host_ctrl.stat_idle_cycles;
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
-      if (host_ctrl.error)
+      if (host_ctrl.error) {
         for (auto& n : host_nets) n.status = host_ctrl.error;
+        note_error(host_ctrl);
+      }
     } else {
       one(0, unsigned(progs.size()));
     }
@@ -899,6 +903,18 @@ struct Runner {
   }
 
   void set_deadline(cudaStream_t st, uint64_t timeout_ms);
+
+  // What the device said about its first error (for the error message).
+  std::string error_detail;
+  void note_error(const dev::Ctrl& h) {
+    if (!error_detail.empty()) return;
+    if (h.error == HVM64_ERR_TIMEOUT)
+      error_detail = h.error_info == 0 ? " (a bounded wait on a locked heap word gave up)"
+                                       : " (the run deadline, tuning timeout_ms, passed)";
+    else
+      error_detail = " (net " + std::to_string(h.error_net) + ")";
+  }
+  std::string error_message(int code) const { return std::string(status_name(code)) + error_detail; }
 
   // A persistent run as one CUDA graph: net records, control block, queue
   // init, deadline, launch parameters, boot and reduce, captured once per
@@ -1418,7 +1434,7 @@ int hvm64_net_normal(hvm64_net* net, const hvm64_tuning* t, hvm64_rewrites* out,
   if (rc) return rc;
   const auto& s = net->r.host_nets[0];
   if (out) *out = hvm64_rewrites{s.rw[0], s.rw[1], s.rw[2], s.rw[3], s.rw[4]};
-  if (s.status) return hvm::set_error(s.status, hvm::status_name(s.status));
+  if (s.status) return hvm::set_error(s.status, net->r.error_message(s.status));
   return HVM64_OK;
 }
 int hvm64_net_readback(hvm64_net* net, char* buf, size_t cap, size_t* len) {
@@ -1470,7 +1486,7 @@ int hvm64_batch_normal(hvm64_batch* b, int mode, const hvm64_tuning* t, hvm64_re
     if (status) status[i] = s.status;
     if (s.status && !worst) worst = s.status;
   }
-  if (worst) return hvm::set_error(worst, hvm::status_name(worst));
+  if (worst) return hvm::set_error(worst, b->r.error_message(worst));
   return HVM64_OK;
 }
 int hvm64_batch_readback(hvm64_batch* b, uint32_t i, char* buf, size_t cap, size_t* len) {
