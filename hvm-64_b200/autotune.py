@@ -18,7 +18,7 @@ SPACE = {
     "blocks_per_sm": (0, 6, 4),
     "chunk_nodes": (0, 4096),
     "donate_min": (0, 32, 128),
-    "queue_slots_log2": (0, 18),
+    "queue_slots_log2": (0, 18, 22),
 }
 ORDER = ("blocks_per_sm", "chunk_nodes", "donate_min", "queue_slots_log2")
 

@@ -694,6 +694,13 @@ const char* status_name(int s) {
 
 }  // namespace
 
+// Default redex-queue capacity: 2^20 slots (570 MB).  A warp whose stack is
+// full ships redexes to the queue one per slot in the middle of a step, and a
+// warp that finds the queue full waits for consumers; when every warp waits
+// like that at once the run stops with TIMEOUT, so the queue is sized for
+// bursts from Defs that create many redexes at once.
+constexpr unsigned DEFAULT_QLOG2 = 20;
+
 // A set of nets reduced together on the current device.
 struct Runner {
   Book book;
@@ -797,7 +804,7 @@ struct Runner {
   void run(int mode, const hvm64_tuning* tp, double* device_ms) {
     hvm64_tuning t{};
     if (tp) t = *tp;
-    unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : 16;
+    unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : DEFAULT_QLOG2;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
     h2d = d2h = 0;
     error_detail.clear();
@@ -909,8 +916,10 @@ struct Runner {
   void note_error(const dev::Ctrl& h) {
     if (!error_detail.empty()) return;
     if (h.error == HVM64_ERR_TIMEOUT)
-      error_detail = h.error_info == 0 ? " (a bounded wait on a locked heap word gave up)"
-                                       : " (the run deadline, tuning timeout_ms, passed)";
+      error_detail = h.error_info == 0
+                         ? " (a bounded wait gave up: a locked heap word, or a full redex queue; "
+                           "a larger tuning queue_slots_log2 helps the latter)"
+                         : " (the run deadline, tuning timeout_ms, passed)";
     else
       error_detail = " (net " + std::to_string(h.error_net) + ")";
   }
@@ -1166,7 +1175,7 @@ struct Server {
     nslots = slots;
     out_cap = out_pairs;
     req_cap = 2 * slots + 16;
-    unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : 16;
+    unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : DEFAULT_QLOG2;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
     size_t qn = size_t(1) << qlog2;
     heap.alloc(heap_bytes / 8);
