@@ -1,6 +1,7 @@
 """Build recipe for the B200 reducer (nvcc for sm_100a + g++ for the host layer).
 
-    python hvm-64_b200/build.py          # builds build/libhvm64.so and build/hvm64
+    python hvm-64_b200/build.py          # builds build/libhvm64.so, build/hvm64 (CLI)
+                                         # and build/hvm64_atomic_peak
 
 Outputs stay in-tree (hvm-64_b200/build/) so they travel with the repository
 snapshot to the GPU machine.
@@ -18,6 +19,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(OUT, "libhvm64.so")
 CLI = os.path.join(OUT, "hvm64")
+PEAK = os.path.join(OUT, "hvm64_atomic_peak")  # L2 atomic-rate microbenchmark
 
 SOURCES = ["hvm64.cu", "host.cpp", "host.hpp", "device.cuh", "num.h", "cli.cpp"]
 
@@ -50,6 +52,9 @@ def build(force=False, verbose=False):
         if verbose:
             sys.stderr.write(log)
         _run([NVCC, *ARCH, "-shared", "-o", LIB, dev_o, host_o, "-lcudart"])
+    peak_src = os.path.join(CSRC, "atomic_peak.cu")
+    if os.path.exists(peak_src) and (force or _stale(PEAK, [peak_src, __file__])):
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", peak_src, "-o", PEAK])
     if os.path.exists(os.path.join(CSRC, "cli.cpp")) and (force or _stale(CLI, deps + [LIB])):
         _run(["g++", "-std=c++20", "-O2", "-I", INC, os.path.join(CSRC, "cli.cpp"), "-o", CLI,
               "-L", OUT, "-lhvm64", "-Wl,-rpath,$ORIGIN"])
