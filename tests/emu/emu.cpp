@@ -213,6 +213,14 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
         with_big_stack([&] { g = readback_pairs(book, reinterpret_cast<const uint64_t*>(pairs.data()), n,
                                                 E.heap.size(), E.nets[0].root); });
         if (g != txt) throw Error(HVM64_ERR_BAD_INPUT, "gathered readback differs: " + g.substr(0, 80));
+        // out of order (the reader's address map instead of its cursor)
+        for (size_t i = 0; i + 1 < n; i += 2) {
+          std::swap(pairs[2 * i], pairs[2 * (i + 1)]);
+          std::swap(pairs[2 * i + 1], pairs[2 * (i + 1) + 1]);
+        }
+        with_big_stack([&] { g = readback_pairs(book, reinterpret_cast<const uint64_t*>(pairs.data()), n,
+                                                E.heap.size(), E.nets[0].root); });
+        if (g != txt) throw Error(HVM64_ERR_BAD_INPUT, "shuffled gathered readback differs: " + g.substr(0, 80));
       }
     }
     *out_text = strdup(txt.c_str());
