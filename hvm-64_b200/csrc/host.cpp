@@ -4,6 +4,7 @@
 #include <pthread.h>
 
 #include <algorithm>
+#include <atomic>
 #include <charconv>
 #include <cmath>
 #include <cstring>
@@ -825,6 +826,51 @@ std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npair
   r.npairs = npairs;
   r.wire(root);
   return r.o;
+}
+
+std::vector<ReadbackOut> readback_pairs_many(const Book& book, const uint64_t* pairs, const uint64_t* offsets,
+                                             const unsigned* counts, const uint64_t* roots, size_t n,
+                                             uint64_t heap_words, unsigned threads) {
+  std::vector<ReadbackOut> out(n);
+  std::atomic<size_t> next{0};
+  struct Job {
+    const Book* book;
+    const uint64_t *pairs, *offsets, *roots;
+    const unsigned* counts;
+    size_t n;
+    uint64_t heap_words;
+    std::vector<ReadbackOut>* out;
+    std::atomic<size_t>* next;
+  } job{&book, pairs, offsets, roots, counts, n, heap_words, &out, &next};
+  auto work = [](void* p) -> void* {
+    Job* j = static_cast<Job*>(p);
+    for (;;) {
+      size_t i = j->next->fetch_add(1);
+      if (i >= j->n) break;
+      ReadbackOut& r = (*j->out)[i];
+      if (j->counts[i] == ~0u) continue;  // not gathered: the caller reads it back another way
+      try {
+        r.text = readback_pairs(*j->book, j->pairs + 2 * j->offsets[i], j->counts[i], j->heap_words, j->roots[i]);
+        r.ok = true;
+      } catch (std::exception& e) {
+        r.error = e.what();
+      }
+    }
+    return nullptr;
+  };
+  threads = std::max(1u, std::min<unsigned>(threads, unsigned(std::max<size_t>(n, 1))));
+  std::vector<pthread_t> ts;
+  pthread_attr_t attr;
+  pthread_attr_init(&attr);
+  pthread_attr_setstacksize(&attr, size_t(256) << 20);  // deep normal forms recurse
+  for (unsigned t = 0; t < threads; t++) {
+    pthread_t th;
+    if (pthread_create(&th, &attr, work, &job) == 0) ts.push_back(th);
+  }
+  pthread_attr_destroy(&attr);
+  if (ts.empty()) work(&job);  // no thread could start: do it here
+  for (auto th : ts) pthread_join(th, nullptr);
+  return out;
 }
 
 void with_big_stack(const std::function<void()>& f) {

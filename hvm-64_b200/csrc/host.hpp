@@ -129,6 +129,16 @@ struct Book {
 // (Host::readback, host/src/readback.rs:23-87).  Redirect chains (Red ports
 // left by concurrent linking) are followed to the live endpoint.
 std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root);
+// Many nets' normal forms from gathered pairs at once, on `threads` host
+// threads: net i's pairs start at pair offsets[i] and number counts[i]
+// (~0u: not gathered, left empty).  A net that fails keeps its message.
+struct ReadbackOut {
+  bool ok = false;
+  std::string text, error;
+};
+std::vector<ReadbackOut> readback_pairs_many(const Book& book, const uint64_t* pairs, const uint64_t* offsets,
+                                             const unsigned* counts, const uint64_t* roots, size_t n,
+                                             uint64_t heap_words, unsigned threads);
 // The same from the (address, word) pairs a serving reducer gathered.
 std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npairs, uint64_t heap_words,
                            uint64_t root);

@@ -24,6 +24,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device.cuh"
@@ -1084,19 +1085,23 @@ struct Runner {
     if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
     d2h += size_t(n) * 4 + 16 * tot;
     h2d += size_t(n) * 8;
+    // Every gathered net's text at once, on the host's cores.
+    std::vector<uint64_t> roots(n);
+    for (unsigned i = 0; i < n; i++) roots[i] = host_nets[i].root;
+    unsigned hw = std::thread::hardware_concurrency();
+    gtext = readback_pairs_many(book, gpairs.data(), goff.data(), gcount.data(), roots.data(), n, heap_bytes / 8,
+                                std::max(1u, std::min(hw ? hw : 1u, 16u)));
     pairs_valid = true;
   }
+  std::vector<ReadbackOut> gtext;
 
   std::string readback(unsigned i) {
     if (!reduced) throw Error(HVM64_ERR_BAD_INPUT, "net not reduced yet");
     if (host_nets[i].status) throw Error(host_nets[i].status, status_name(host_nets[i].status));
     if (!pairs_valid) gather_all();
     if (gcount[i] != ~0u) {
-      std::string out;
-      with_big_stack([&] {
-        out = hvm::readback_pairs(book, gpairs.data() + 2 * goff[i], gcount[i], heap_bytes / 8, host_nets[i].root);
-      });
-      return out;
+      if (!gtext[i].ok) throw Error(HVM64_ERR_BAD_INPUT, gtext[i].error);
+      return gtext[i].text;
     }
     if (!image_valid) {
       // Copy the used part of the heap (everything below the bump pointer).

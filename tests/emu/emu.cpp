@@ -221,6 +221,17 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
         with_big_stack([&] { g = readback_pairs(book, reinterpret_cast<const uint64_t*>(pairs.data()), n,
                                                 E.heap.size(), E.nets[0].root); });
         if (g != txt) throw Error(HVM64_ERR_BAD_INPUT, "shuffled gathered readback differs: " + g.substr(0, 80));
+        // many nets at once on several host threads (here: the same net 8 times,
+        // plus one not gathered)
+        std::vector<uint64_t> offs(9, 0), roots(9, E.nets[0].root);
+        std::vector<unsigned> counts(9, n);
+        counts[4] = ~0u;
+        auto many = readback_pairs_many(book, reinterpret_cast<const uint64_t*>(pairs.data()), offs.data(),
+                                        counts.data(), roots.data(), 9, E.heap.size(), 4);
+        for (size_t i = 0; i < 9; i++) {
+          if (i == 4 ? (many[i].ok || !many[i].text.empty()) : (!many[i].ok || many[i].text != txt))
+            throw Error(HVM64_ERR_BAD_INPUT, "parallel gathered readback differs at " + std::to_string(i));
+        }
       }
     }
     *out_text = strdup(txt.c_str());
