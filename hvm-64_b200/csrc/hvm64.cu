@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
           cur = int(admitted - 1);
           c.net = unsigned(cur);
           bot = 0;
+          __syncwarp();  // lane 0's boot pushes are in shared memory before the others read the count
           top = min(W.ring_cnt, unsigned(SCAP - HEADROOM));
           continue;
         }
