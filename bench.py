@@ -57,6 +57,28 @@ def algorithmic_bytes(counts, stats):
             counts["oper"] * BYTES["oper"] + dref_bytes(stats["dref_nodes"], stats["dref_links"], counts["dref"]))
 
 
+# Global atomics per interaction of the same model (exchange or CAS); a Def
+# call takes about one per link to its argument.
+ATOMICS = {"anni": 8, "comm22": 8, "comm02": 4, "oper": 2}
+
+
+def algorithmic_atomics(counts, stats):
+    comm22 = stats["comm22"]
+    comm02 = counts["comm"] - comm22
+    return (counts["anni"] * ATOMICS["anni"] + comm22 * ATOMICS["comm22"] + comm02 * ATOMICS["comm02"] +
+            counts["oper"] * ATOMICS["oper"] + stats["dref_links"])
+
+
+def atomic_peak():
+    """The measured L2 atomic rate (ops/s), if the microbenchmark's line was
+    saved beside the measured peaks; else None."""
+    try:
+        p = json.load(open(os.path.join(ROOT, "profiles", "atomic_peak.json")))
+        return min(float(p["atomic_exch_gops"]), float(p["atomic_cas_gops"])) * 1e9
+    except Exception:
+        return None
+
+
 def peaks():
     try:
         p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -364,6 +386,8 @@ def main():
     # device time (CUDA events the library records on its launching stream)
     hbm, peak_kind = peaks()
     alg = algorithmic_bytes(counts, stats)
+    atoms = algorithmic_atomics(counts, stats)
+    arate = atomic_peak()
     kms = statistics.mean(kernel_ms)
     achieved = alg / (kms / 1000.0) / 1e9
     traffic = TRAFFIC_PER_INTERACTION * total_per_step if TRAFFIC_PER_INTERACTION else None
@@ -375,7 +399,9 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",
                      "kernel": "reduce_kernel (+ boot_kernel) device time per launch", "kernel_ms": kms,
-                     "algorithmic_bytes": alg},
+                     "algorithmic_bytes": alg, "algorithmic_atomics": atoms,
+                     "atomic_rate_ops": arate,
+                     "atomic_frac": (atoms / (kms / 1000.0)) / arate if arate else None},
         "gpu_launches": 4 * args.steps,
         "tuning": {"knobs": {k: getattr(tune, k) for k in ("blocks_per_sm", "chunk_nodes", "donate_min",
                                                             "queue_slots_log2")},
