@@ -854,6 +854,8 @@ std::vector<ReadbackOut> readback_pairs_many(const Book& book, const uint64_t* p
         r.ok = true;
       } catch (std::exception& e) {
         r.error = e.what();
+      } catch (...) {
+        r.error = "readback failed";
       }
     }
     return nullptr;
