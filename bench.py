@@ -224,6 +224,10 @@ def serve_leg(args, hvm64):
         last = 0.0
         while len(lat) < len(names):
             now = time.perf_counter() - t_start
+            if now > arr[-1] + args.serve_wait_s:
+                sv.close()
+                raise RuntimeError(f"serving: {len(names) - len(lat)} requests unfinished "
+                                   f"{args.serve_wait_s} s after the last arrival")
             busy = False
             while i < len(names) and arr[i] <= now and inflight < args.serve_slots:
                 owner[sv.submit(names[i])] = i
@@ -303,6 +307,8 @@ def main():
     ap.add_argument("--device-only", action="store_true", help="skip the plain, e2e, serving and CPU legs")
     ap.add_argument("--serve-requests", type=int, default=96, help="requests per offered load (0: no serving leg)")
     ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--serve-wait-s", type=float, default=120.0,
+                    help="give up on a load this long after its last arrival")
     ap.add_argument("--autotune", type=int, default=1, help="pick the launch knobs on a sample first (0: defaults)")
     ap.add_argument("--tune-sample", type=int, default=1024)
     args = ap.parse_args()
@@ -461,7 +467,10 @@ def main():
 
         if rank == 0 and args.serve_requests > 0:
             del batch
-            out["serving"] = serve_leg(args, hvm64)
+            try:
+                out["serving"] = serve_leg(args, hvm64)
+            except Exception as e:  # the serving leg must not cost the benchmark line
+                out["serving"] = {"error": f"{type(e).__name__}: {e}"}
 
         if rank == 0:
             t, n = pow2_threads()
