@@ -474,9 +474,13 @@ def main():
 
         if rank == 0:
             t, n = pow2_threads()
-            v, desc = cpu_baseline(entries, args.cpu_budget, t)
-            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": t, "kind": "port", "sample": desc,
-                                   "host_cpus": n}
+            try:
+                v, desc = cpu_baseline(entries, args.cpu_budget, t)
+                out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": t, "kind": "port", "sample": desc,
+                                       "host_cpus": n}
+            except Exception as e:
+                out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": t, "kind": "port",
+                                       "error": f"{type(e).__name__}: {e}"}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
