@@ -137,6 +137,10 @@ struct Params {
   const DevInstr* __restrict__ instrs;
   const ull* __restrict__ labbits;
   unsigned ndefs;
+  // per-warp overflow stacks: warp g of the reducer grid owns
+  // spill[2 * spill_cap * g ...] (spill_cap redexes); null: none
+  unsigned spill_cap;
+  ull* spill;
   // serving (all zero for a batch run)
   unsigned serve;
   const ServeReq* req;         // device ring of req_cap requests
@@ -145,10 +149,22 @@ struct Params {
   unsigned req_cap, out_cap;
 };
 
-// The run's parameters: CUDA constant memory (set before each launch), or a
-// plain global in the host emulation.
+// The run's parameters.  On the GPU every kernel receives them as a
+// by-value (__grid_constant__) argument and copies them into this per-block
+// shared-memory variable before anything else, so launches of different
+// handles on one device never see each other's parameters.  The host
+// emulation uses a plain global.
 #ifdef __CUDACC__
-__constant__ Params g_P;
+__shared__ Params g_P;
+// Every kernel's first statement: all threads of the block call it.
+__device__ __forceinline__ void load_params(const Params& P) {
+  constexpr unsigned W = sizeof(Params) / 8;
+  static_assert(sizeof(Params) % 8 == 0, "Params is copied in 8-byte words");
+  const ull* src = reinterpret_cast<const ull*>(&P);
+  ull* dst = reinterpret_cast<ull*>(&g_P);
+  for (unsigned i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
 #else
 inline Params g_P;
 #endif
@@ -319,7 +335,9 @@ struct WarpSmem {
   ull bnext[32], bend[32];    // per lane: pre-LOCKed bump chunk [bnext, bend), node indices
   unsigned allocs[32];        // per lane: nodes allocated (for the DREF statistics)
   unsigned ring_base;         // this step's pushes go to stack slots ring_base + k ...
-  unsigned ring_cap;          // ... for k < ring_cap
+  unsigned ring_cap;          // ... for k < ring_cap; push k >= ring_cap goes to the overflow stack
+  ull* sp;                    // this warp's overflow stack in HBM (null: none; pushes go to the queue)
+  unsigned sp_n, sp_cap;      // redexes in it between steps, and its capacity
   int pool_cap;               // 0: no reuse pool (reclaimed nodes go to `ovf`)
 #ifdef HVM_PROFILE_OPS
   ull prof[32];               // profiling build: op counts and wait cycles, cycles per rule
@@ -384,8 +402,9 @@ HVM_COLD uint32_t binary_op(unsigned net, uint32_t a, uint32_t op, uint32_t b) {
   if (e) run_fail(net, HVM64_ERR_DIV0, net);
   return r;
 }
-// The warp's stack had no room: the platform driver ships the redex to
-// shared work (the CUDA driver: a one-redex queue slot).
+// Neither the warp's stack nor its overflow stack had room: the platform
+// driver ships the redex to shared work (the CUDA driver: a one-redex queue
+// slot, or HVM64_ERR_QUEUE when the queue is full -- it never waits).
 HVM_COLD void push_overflow(unsigned net, ull a, ull b);
 // Pop the rare overflow free list / take a new pre-LOCKed bump chunk.
 struct Refill {
@@ -570,16 +589,48 @@ HVM_COLD void half_free(const Ctx& c, ull a) {
 }
 
 // ---- redex pushes (linker.rs:70-85) -----------------------------------------
+// The reference's queue is an unbounded vector (linker.rs:308-344); here a
+// step's k-th push goes to the warp's shared-memory stack while it has room,
+// then to the warp's private overflow stack in HBM (slot sp_n + k - ring_cap),
+// then to the global queue.  None of these waits for anyone.
+HVM_COLD void push_spill(const Ctx& c, ull a, ull b, unsigned j) {
+  unsigned i = c.W->sp_n + j;
+  if (c.W->sp && i < c.W->sp_cap) {
+    c.W->sp[2 * ull(i)] = a;
+    c.W->sp[2 * ull(i) + 1] = b;
+    return;
+  }
+  push_overflow(c.net, a, b);
+}
 HVM_INL void push(const Ctx& c, ull a, ull b) {
   unsigned cap = c.W->ring_cap;
-  unsigned k = cap ? agg_add_u32(&c.W->ring_cnt, 1u) : 0u;
+  unsigned k = agg_add_u32(&c.W->ring_cnt, 1u);
   if (k < cap) {
     unsigned i = (c.W->ring_base + k) & unsigned(SCAP - 1);
     c.W->stk[2 * i] = a;
     c.W->stk[2 * i + 1] = b;
   } else {
-    push_overflow(c.net, a, b);
+    push_spill(c, a, b, k - cap);
   }
+}
+// After a step that pushed `cnt` redexes (the value of ring_cnt): how many of
+// them went to the overflow stack (the rest of those past ring_cap went to
+// the queue).
+HVM_INL unsigned spilled_of(const WarpSmem* W, unsigned cnt) {
+  if (cnt <= W->ring_cap || !W->sp) return 0;
+  unsigned over = cnt - W->ring_cap, room = W->sp_cap - W->sp_n;
+  return over < room ? over : room;
+}
+// Upper bound on the redexes one interaction of rule class `cls` pushes
+// (redex_class codes): an instruction of a Def pushes at most one (each
+// link resolves to at most one active pair); a Def call that commutes
+// instead (def.rs:182-184) pushes two, comm22 four, the other rules fewer.
+HVM_INL unsigned pushes_bound(unsigned cls) {
+  if (cls >= 64 && cls - 64 < g_P.ndefs) {
+    unsigned r = g_P.defs[cls - 64].redexes;
+    return r > 4 ? r : 4;
+  }
+  return 4;
 }
 HVM_INL void redux(const Ctx& c, ull a, ull b) {
   if (skippable(a) && skippable(b)) count(c, RW_ERAS);

@@ -34,12 +34,13 @@ namespace dev {
 
 // ---- global redex queue --------------------------------------------------------
 // Single-thread reservation; data movement may be done by the whole warp.
-__device__ bool q_reserve_push(unsigned net, ull& pos, bool must) {
+// Never waits for a consumer: a full queue (or a reservation that keeps
+// losing its CAS) returns false and the caller keeps the work.
+__device__ bool q_reserve_push(ull& pos) {
   Ctrl* C = g_P.ctrl;
   ull mask = C->q_mask;
   pos = ld_gpu(&C->q_tail);
-  unsigned it = 0;
-  for (;;) {
+  for (int tries = 0; tries < 256; tries++) {
     Slot* s = &g_P.q[pos & mask];
     long long dif = (long long)ld_gpu(&s->seq) - (long long)pos;
     if (dif == 0) {
@@ -47,16 +48,12 @@ __device__ bool q_reserve_push(unsigned net, ull& pos, bool must) {
       if (old == pos) return true;
       pos = old;
     } else if (dif < 0) {
-      if (!must) return false;  // full
-      pos = ld_gpu(&C->q_tail);
+      return false;  // full
     } else {
       pos = ld_gpu(&C->q_tail);
     }
-    if (!run_spin(net, it)) {
-      if (must && !run_failed()) run_fail(net, HVM64_ERR_QUEUE, pos);
-      return false;
-    }
   }
+  return false;
 }
 __device__ void q_publish(ull pos) {
   __threadfence();
@@ -86,12 +83,17 @@ __device__ void q_release(ull pos) {
   st_gpu(&g_P.q[pos & g_P.ctrl->q_mask].seq, pos + g_P.ctrl->q_mask + 1);
 }
 
-// The warp's stack is full: ship one redex as its own slot (rare: each step
-// starts with HEADROOM free stack slots).
+// Neither stack of the pushing warp had room (or the pusher has no overflow
+// stack: the boot kernel): ship one redex as its own slot.  A full queue
+// ends the run with HVM64_ERR_QUEUE instead of waiting for consumers, which
+// could all be waiting the same way.
 __device__ __noinline__ void push_overflow(unsigned net, ull a, ull b) {
-  atomicAdd(reinterpret_cast<ull*>(&g_P.nets[net].pending), 1ull);
   ull pos;
-  if (!q_reserve_push(net, pos, true)) return;
+  if (!q_reserve_push(pos)) {
+    run_fail(net, HVM64_ERR_QUEUE, 0);
+    return;
+  }
+  atomicAdd(reinterpret_cast<ull*>(&g_P.nets[net].pending), 1ull);
   Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
   st_gpu(reinterpret_cast<ull*>(&s->net), (1ull << 32) | net);
   st_gpu(&s->r[0], a);
@@ -102,31 +104,51 @@ __device__ __noinline__ void push_overflow(unsigned net, ull a, ull b) {
 
 __device__ __forceinline__ ull shfl(ull v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 
-// Warp-cooperative: move the `cnt` oldest redexes of the warp's stack into a
-// queue slot.  Returns false if the queue had no room (only when !must).
-__device__ bool donate(ull* S, unsigned& bot, unsigned cnt, int cur, bool must) {
+// Warp-cooperative: publish one queue slot of net `cur` holding the redexes
+// (ra, rb) of lanes < cnt.  Returns false, changing nothing, when the queue
+// has no room.
+__device__ bool donate_vals(ull ra, ull rb, unsigned cnt, int cur) {
   const unsigned lane = threadIdx.x & 31;
   ull pos = 0;
   int ok = 0;
   if (lane == 0) {
-    atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), 1ull);
-    ok = q_reserve_push(unsigned(cur), pos, must) ? 1 : 0;
-    if (!ok) atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), ~0ull);
+    ok = q_reserve_push(pos) ? 1 : 0;
+    if (ok) atomicAdd(reinterpret_cast<ull*>(&g_P.nets[cur].pending), 1ull);
   }
   ok = __shfl_sync(0xffffffffu, ok, 0);
   if (!ok) return false;
   pos = shfl(pos, 0);
   Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
   if (lane < cnt) {
-    unsigned k = (bot + lane) & (SCAP - 1);
-    st_gpu(&s->r[2 * lane], S[2 * k]);
-    st_gpu(&s->r[2 * lane + 1], S[2 * k + 1]);
+    st_gpu(&s->r[2 * lane], ra);
+    st_gpu(&s->r[2 * lane + 1], rb);
   }
   if (lane == 0) st_gpu(reinterpret_cast<ull*>(&s->net), (ull(cnt) << 32) | unsigned(cur));
   __threadfence();
   __syncwarp();
   if (lane == 0) q_publish(pos);
+  return true;
+}
+// The `cnt` oldest redexes of the warp's shared-memory stack into a slot.
+__device__ bool donate(const ull* S, unsigned& bot, unsigned cnt, int cur) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned k = (bot + lane) & (SCAP - 1);
+  ull ra = lane < cnt ? S[2 * k] : 0, rb = lane < cnt ? S[2 * k + 1] : 0;
+  if (!donate_vals(ra, rb, cnt, cur)) return false;
   bot += cnt;
+  return true;
+}
+// The 32 newest redexes of the warp's overflow stack into a slot.
+__device__ bool donate_spill(WarpSmem& W, int cur) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned n = W.sp_n;
+  if (n < 32u) return false;
+  ull i = n - 32u + lane;
+  ull ra = W.sp[2 * i], rb = W.sp[2 * i + 1];
+  if (!donate_vals(ra, rb, 32u, cur)) return false;
+  __syncwarp();
+  if (lane == 0) W.sp_n = n - 32u;
+  __syncwarp();
   return true;
 }
 
@@ -177,7 +199,9 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
 // or writes its net's pairs at offs[i].  A net whose walk overflows the
 // stack gets count ~0u and is read back from a heap image instead.
 constexpr unsigned GATHER_STACK = 256;
-__global__ void gather_kernel(unsigned n, unsigned* counts, const ull* offs, ull* out) {
+__global__ void gather_kernel(const __grid_constant__ Params P, unsigned n, unsigned* counts, const ull* offs,
+                              ull* out) {
+  load_params(P);
   unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   ull stk[GATHER_STACK];
@@ -269,7 +293,8 @@ constexpr int QW = HVM_QW;  // selection window: 32 * QW newest redexes
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
-__global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
+__global__ void __launch_bounds__(THREADS, 7) reduce_kernel(const __grid_constant__ Params P) {
+  load_params(P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
@@ -290,6 +315,10 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
     W.pool_cap = POOL;
     W.ring_base = 0;
     W.ring_cap = 0;
+    const ull gw = ull(blockIdx.x) * WARPS + (threadIdx.x >> 5);
+    W.sp = g_P.spill ? g_P.spill + 2ull * g_P.spill_cap * gw : nullptr;
+    W.sp_cap = g_P.spill ? g_P.spill_cap : 0u;
+    W.sp_n = 0;
     W.st_steps = W.st_lanes = W.st_busy = W.st_idle = W.st_lane_sum = W.st_lane_max = 0;
   }
   __syncwarp();
@@ -309,6 +338,25 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       int err = 0;
       if (lane == 0) err = ld_gpu32(&C->error);
       if (__shfl_sync(0xffffffffu, err, 0)) break;
+    }
+
+    // Refill a low stack from the overflow stack (its newest redexes), so
+    // steps stay full and the warp keeps the net while either holds work.
+    {
+      const unsigned spn = W.sp_n;
+      if (spn && top - bot < 64u) {
+        unsigned m = min(spn, unsigned(SCAP - HEADROOM) - (top - bot));
+        const ull* src = W.sp + 2ull * (spn - m);
+        for (unsigned i = lane; i < m; i += 32) {
+          unsigned k = (top + i) & (SCAP - 1);
+          S[2 * k] = src[2 * i];
+          S[2 * k + 1] = src[2 * i + 1];
+        }
+        top += m;
+        __syncwarp();
+        if (lane == 0) W.sp_n = spn - m;
+        __syncwarp();
+      }
     }
 
     if (top == bot) {
@@ -367,7 +415,14 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
           c.net = unsigned(cur);
           bot = 0;
           __syncwarp();  // lane 0's boot pushes are in shared memory before the others read the count
-          top = min(W.ring_cnt, unsigned(SCAP - HEADROOM));
+          {
+            const unsigned cnt = W.ring_cnt;
+            top = min(cnt, W.ring_cap);
+            const unsigned spilled = spilled_of(&W, cnt);
+            __syncwarp();
+            if (lane == 0) W.sp_n += spilled;
+            __syncwarp();
+          }
           continue;
         }
         // (a serving reducer naps at most 8 us: new requests wait on it)
@@ -419,9 +474,22 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       if (__shfl_sync(0xffffffffu, late, 0)) break;
     }
 
-    // Keep HEADROOM slots free for this step's new redexes.
+    // Keep HEADROOM slots free for this step's new redexes: the oldest
+    // redexes move to the overflow stack, or to the queue; if neither has
+    // room the step's pushes overflow instead (nothing waits).
     while ((top - bot) > unsigned(SCAP - HEADROOM)) {
-      if (!donate(S, bot, 32u, cur, true)) break;
+      const unsigned spn = W.sp_n;
+      if (W.sp && spn + 32u <= W.sp_cap) {
+        unsigned k = (bot + lane) & (SCAP - 1);
+        W.sp[2ull * (spn + lane)] = S[2 * k];
+        W.sp[2ull * (spn + lane) + 1] = S[2 * k + 1];
+        bot += 32u;
+        __syncwarp();
+        if (lane == 0) W.sp_n = spn + 32u;
+        __syncwarp();
+      } else if (!donate(S, bot, 32u, cur)) {
+        break;
+      }
       if (lane == 0) atomicAdd(&C->stat_spilled, 1ull);
     }
 
@@ -461,6 +529,15 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       um[q] = __ballot_sync(0xffffffffu, su[q]);
     }
     unsigned n = min(nsel, 32u);
+    // Run only as many lanes as the stacks can take the pushes of (a lane of
+    // a Def call pushes at most the Def's bound); the rest stay selected-out
+    // and go back on the stack below.
+    const unsigned nsel32 = n;
+    {
+      unsigned free_slots = unsigned(SCAP) - (top - bot) + n + (W.sp ? W.sp_cap - W.sp_n : 0u);
+      unsigned lim = free_slots / pushes_bound(key);
+      n = max(1u, min(n, lim));
+    }
     unsigned base = top - w;
     __syncwarp();
     // Entries that stay keep their relative depth (older quarters lower; in a
@@ -480,6 +557,15 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       below += unsigned(__popc(um[q]));
     }
     top = base + below;
+    if (n < nsel32) {  // selected beyond the lane cap: back on the stack
+      __syncwarp();
+      if (lane >= n && lane < nsel32) {
+        unsigned k = (top + lane - n) & (SCAP - 1);
+        S[2 * k] = W.sel[2 * lane];
+        S[2 * k + 1] = W.sel[2 * lane + 1];
+      }
+      top += nsel32 - n;
+    }
     if (lane == 0) {
       W.ring_cnt = 0;
       W.ring_base = top;
@@ -530,8 +616,11 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       }
     }
     {
-      unsigned pushed = min(W.ring_cnt, unsigned(SCAP) - (top - bot));
-      top += pushed;
+      const unsigned cnt = W.ring_cnt;
+      top += min(cnt, W.ring_cap);
+      const unsigned spilled = spilled_of(&W, cnt);
+      __syncwarp();
+      if (lane == 0) W.sp_n += spilled;
     }
     fold_counts(W);
     // Nodes reclaimed in this step become allocatable after a fence.
@@ -556,19 +645,26 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
       __syncwarp();
     }
 
-    // Share the oldest work when other warps are starving.
-    if (top - bot >= unsigned(C->donate_min) && ((step & 7) == 0)) {
+    // Share work when other warps are starving: the overflow stack first,
+    // then the oldest half of the shared-memory stack (at most four slots
+    // per check).
+    if (top - bot + W.sp_n >= unsigned(C->donate_min) && ((step & 7) == 0)) {
       int give = 0;
       if (lane == 0) {
         long long h = ld_gpu64s(&C->hungry);
         long long queued = (long long)(ld_gpu(&C->q_tail) - ld_gpu(&C->q_head));
         give = h > 0 && queued < h;
       }
-      // Give up to half the stack (at most four slots) per check.
-      unsigned chunks = __shfl_sync(0xffffffffu, give, 0) ? min((top - bot) / 64u, 4u) : 0u;
-      for (unsigned k = 0; k < chunks; k++) {
-        if (!donate(S, bot, 32u, cur, false)) break;
-        if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
+      if (__shfl_sync(0xffffffffu, give, 0)) {
+        unsigned k = 0;
+        for (; k < 4u && W.sp_n >= 32u; k++) {
+          if (!donate_spill(W, cur)) break;
+          if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
+        }
+        for (unsigned chunks = min((top - bot) / 64u, 4u - k); chunks; chunks--) {
+          if (!donate(S, bot, 32u, cur)) break;
+          if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
+        }
       }
     }
   }
@@ -587,50 +683,66 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel() {
   }
 }
 
-// One thread per net: allocate the root, run the boot program against it
+// One warp per net (lane 0 does the work, its state in shared memory like
+// the reducer's): allocate the root, run the boot program against it
 // (Net::boot / Host::encode_net), then wrap the root in an expansion agent
-// (Net::expand, runtime/src/net.rs:65-69).  Redexes go to the global queue in
-// slots of up to 32.
-__global__ void boot_kernel(unsigned first, unsigned count) {
-  unsigned i = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= first + count) return;
-  WarpSmem W;  // this thread's private copy (local memory)
-  W.ring_cnt = 0;
-  W.icache_def = ~0u;
-  W.pool_n = W.freed_n = 0;
-  W.pool_cap = 0;
-  W.ring_base = 0;
-  W.ring_cap = CHUNK;
-  for (int k = 0; k < NCOUNT; k++) W.rw[k] = 0;
-  lane_init(&W, 0);
-  Ctx c{&W, 0, i};
-  NetState& ns = g_P.nets[i];
-  ull root = alloc(c);
-  unsigned prog = unsigned(ns.prog);
-  if (prog < g_P.ndefs && !(g_P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
-  // Small Defs use register slots 0, 32, 64, ... of W.regs (lane 0's column).
-  run_def(c, prog, pvar(root));
-  settle(c);
-  root = expand(c, root);
-  settle(c);
-  ns.root = root;
-  unsigned k = min(W.ring_cnt, unsigned(CHUNK));
-  if (k) {
-    atomicAdd(reinterpret_cast<ull*>(&ns.pending), 1ull);
-    ull pos;
-    if (q_reserve_push(i, pos, true)) {
-      Slot* s = &g_P.q[pos & g_P.ctrl->q_mask];
-      st_gpu(reinterpret_cast<ull*>(&s->net), (ull(k) << 32) | i);
-      for (unsigned j = 0; j < 2 * k; j++) st_gpu(&s->r[j], W.stk[j]);
-      q_publish(pos);
+// (Net::expand, runtime/src/net.rs:65-69).  Redexes collect in the warp's
+// stack (SCAP of them; more go out one per queue slot) and the warp
+// publishes them to the global queue in slots of up to 32.
+__global__ void __launch_bounds__(THREADS) boot_kernel(const __grid_constant__ Params P, unsigned first,
+                                                       unsigned count) {
+  load_params(P);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+  const unsigned lane = threadIdx.x & 31;
+  if (lane == 0) {
+    W.icache_def = ~0u;
+    W.pool_n = W.freed_n = 0;
+    W.pool_cap = 0;
+    W.sp = nullptr;
+    W.sp_n = W.sp_cap = 0;
+    lane_init(&W, 0);
+  }
+  const unsigned stride = gridDim.x * WARPS;
+  for (unsigned i = first + blockIdx.x * WARPS + (threadIdx.x >> 5); i < first + count; i += stride) {
+    NetState& ns = g_P.nets[i];
+    if (lane == 0) {
+      W.ring_cnt = 0;
+      W.ring_base = 0;
+      W.ring_cap = SCAP;
+      for (int k = 0; k < NCOUNT; k++) W.rw[k] = 0;
+      Ctx c{&W, 0, i};
+      ull root = alloc(c);
+      unsigned prog = unsigned(ns.prog);
+      if (prog < g_P.ndefs && !(g_P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
+      // Small Defs use register slots 0, 32, 64, ... of W.regs (lane 0's column).
+      run_def(c, prog, pvar(root));
+      settle(c);
+      root = expand(c, root);
+      settle(c);
+      ns.root = root;
     }
+    __syncwarp();
+    const unsigned total = min(W.ring_cnt, unsigned(SCAP));
+    for (unsigned done = 0; done < total; done += unsigned(CHUNK)) {
+      unsigned k = min(total - done, unsigned(CHUNK));
+      ull ra = lane < k ? W.stk[2 * (done + lane)] : 0, rb = lane < k ? W.stk[2 * (done + lane) + 1] : 0;
+      if (!donate_vals(ra, rb, k, int(i))) {
+        if (lane == 0) run_fail(i, HVM64_ERR_QUEUE, 0);
+        break;
+      }
+    }
+    if (lane == 0) {
+      for (int k = 0; k < NCOUNT; k++) {
+        ull v = W.rw[k] + W.cnt[k * 32];
+        W.cnt[k * 32] = 0;
+        if (v) atomicAdd(&ns.rw[k], v);
+      }
+      __threadfence();
+      if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&g_P.ctrl->nets_left), 1ull);
+    }
+    __syncwarp();
   }
-  for (int k = 0; k < NCOUNT; k++) {
-    ull v = W.rw[k] + W.cnt[k * 32];
-    if (v) atomicAdd(&ns.rw[k], v);
-  }
-  __threadfence();
-  if (ld_gpu64s(&ns.pending) > 0) atomicAdd(reinterpret_cast<ull*>(&g_P.ctrl->nets_left), 1ull);
 }
 
 __global__ void set_deadline_kernel(Ctrl* c, ull timeout_ns);
@@ -692,6 +804,35 @@ const char* status_name(int s) {
     case HVM64_ERR_OUTPUT: return "normal form larger than the request's output buffer";
   }
   return "unknown error";
+}
+
+// Resident reducer blocks per SM for a tuning (the occupancy limit when the
+// tuning leaves it at 0).
+int reducer_blocks_per_sm(const hvm64_tuning& t) {
+  CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dev::SMEM_BYTES)));
+  int bps = int(t.blocks_per_sm);
+  if (bps <= 0) {
+    int occ = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
+    bps = std::max(1, occ);
+  }
+  return bps;
+}
+
+// Overflow-stack capacity per reducer warp: a power of two in [256, 8192]
+// redexes, about half the heap's nodes spread over the warps (live redexes
+// hold nodes, so a small heap cannot fill a large overflow stack).
+unsigned spill_cap_for(uint64_t heap_bytes, uint64_t warps) {
+  uint64_t per = heap_bytes / 16 / std::max<uint64_t>(warps, 1) / 2;
+  unsigned c = 256;
+  while (c < 8192 && c < per) c *= 2;
+  return c;
+}
+
+// Boot kernel grid: one warp per net, at most 8 blocks per SM (grid-stride).
+unsigned boot_blocks(unsigned count, int sms) {
+  unsigned b = (count + dev::WARPS - 1) / dev::WARPS;
+  return std::max(1u, std::min(b, unsigned(sms) * 8u));
 }
 
 }  // namespace
@@ -765,26 +906,28 @@ struct Runner {
     p.instrs = d_instrs.p;
     p.labbits = d_labbits.p;
     p.ndefs = unsigned(book.defs.size());
+    p.spill = spill.p;
+    p.spill_cap = spill_cap;
     return p;
   }
 
-  // Reduce nets [first, first+count) (the rest stay untouched).
-  void launch(unsigned first, unsigned count, const hvm64_tuning& t, cudaStream_t st) {
+  // The reducer grid for a tuning, and the warps' overflow stacks sized to it.
+  DevBuf<dev::ull> spill;
+  unsigned spill_cap = 0, grid = 0;
+  void prepare_grid(const hvm64_tuning& t) {
+    grid = unsigned(sms * reducer_blocks_per_sm(t));
+    uint64_t warps = uint64_t(grid) * dev::WARPS;
+    spill_cap = spill_cap_for(heap_bytes, warps);
+    spill.alloc(2 * size_t(spill_cap) * warps);
+  }
+
+  // Reduce nets [first, first+count) (the rest stay untouched); the grid is
+  // prepared (prepare_grid) for this tuning.
+  void launch(unsigned first, unsigned count, cudaStream_t st) {
     dev::Params p = params();
-    unsigned bt = 128;
-    CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, st));
-    dev::boot_kernel<<<(count + bt - 1) / bt, bt, 0, st>>>(first, count);
+    dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, st>>>(p, first, count);
     CU(cudaGetLastError());
-    CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(dev::SMEM_BYTES)));
-    int bps = int(t.blocks_per_sm);
-    if (bps <= 0) {
-      int occ = 0;
-      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS,
-                                                       dev::SMEM_BYTES));
-      bps = std::max(1, occ);
-    }
-    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>();
+    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>(p);
     CU(cudaGetLastError());
   }
 
@@ -815,6 +958,7 @@ struct Runner {
     nets.alloc(progs.size());
     q.alloc(size_t(1) << qlog2);
     upload_book();
+    prepare_grid(t);
     size_t qn = size_t(1) << qlog2;
 
     host_nets.assign(progs.size(), dev::NetState{});
@@ -847,7 +991,7 @@ struct Runner {
       host_ctrl.timeout_ns = timeout_ms * 1000000ull;
       CU(cudaMemcpyAsync(&ctrl.p->timeout_ns, &host_ctrl.timeout_ns, 8, cudaMemcpyHostToDevice, st));
       CU(cudaEventRecord(e0, st));
-      launch(first, count, t, st);
+      launch(first, count, st);
       CU(cudaEventRecord(e1, st));
       CU(cudaEventSynchronize(e1));
       float ms = 0;
@@ -936,17 +1080,14 @@ struct Runner {
   std::vector<uint64_t> gkey;
   dev::Ctrl* pin_ctrl = nullptr;
   dev::NetState* pin_nets = nullptr;
-  dev::Params* pin_params = nullptr;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
     if (pin_ctrl) cudaFreeHost(pin_ctrl);
     if (pin_nets) cudaFreeHost(pin_nets);
-    if (pin_params) cudaFreeHost(pin_params);
     pin_ctrl = nullptr;
     pin_nets = nullptr;
-    pin_params = nullptr;
   }
   ~Runner() {
     drop_graph();
@@ -957,7 +1098,8 @@ struct Runner {
     size_t qn = size_t(1) << qlog2;
     unsigned count = unsigned(progs.size());
     std::vector<uint64_t> key = {t.blocks_per_sm, t.chunk_nodes, t.donate_min, qlog2, t.lane_budget, timeout_ms,
-                                 count, uint64_t(heap.p), uint64_t(q.p), uint64_t(d_defs.p)};
+                                 count, uint64_t(heap.p), uint64_t(q.p), uint64_t(d_defs.p), uint64_t(spill.p),
+                                 spill_cap, grid};
     for (auto p : progs) key.push_back(p);
     if (!gs) CU(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
     if (!gexec || key != gkey) {
@@ -965,7 +1107,6 @@ struct Runner {
       CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_ctrl), sizeof(dev::Ctrl), cudaHostAllocDefault));
       CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_nets), sizeof(dev::NetState) * std::max<size_t>(count, 1),
                        cudaHostAllocDefault));
-      CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_params), sizeof(dev::Params), cudaHostAllocDefault));
       memcpy(pin_nets, host_nets.data(), sizeof(dev::NetState) * count);
       dev::Ctrl c{};
       c.bump = 1;
@@ -979,15 +1120,7 @@ struct Runner {
       c.deadline = ~0ull;
       c.timeout_ns = timeout_ms * 1000000ull;
       *pin_ctrl = c;
-      *pin_params = params();
-      CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(dev::SMEM_BYTES)));
-      int bps = int(t.blocks_per_sm);
-      if (bps <= 0) {
-        int occ = 0;
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
-        bps = std::max(1, occ);
-      }
+      const dev::Params p = params();
       CU(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaSuccess;
@@ -1000,10 +1133,9 @@ struct Runner {
       step(cudaGetLastError());
       dev::set_deadline_kernel<<<1, 1, 0, gs>>>(ctrl.p, c.timeout_ns);
       step(cudaGetLastError());
-      step(cudaMemcpyToSymbolAsync(dev::g_P, pin_params, sizeof(dev::Params), 0, cudaMemcpyHostToDevice, gs));
-      dev::boot_kernel<<<(count + 127) / 128, 128, 0, gs>>>(0, count);
+      dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, gs>>>(p, 0, count);
       step(cudaGetLastError());
-      dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, gs>>>();
+      dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, gs>>>(p);
       step(cudaGetLastError());
       cudaError_t ec = cudaStreamEndCapture(gs, &g);
       if (e == cudaSuccess) e = ec;
@@ -1026,7 +1158,7 @@ struct Runner {
     CU(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    h2d += sizeof(dev::NetState) * count + sizeof(dev::Ctrl) + sizeof(dev::Params);
+    h2d += sizeof(dev::NetState) * count + sizeof(dev::Ctrl);
     return ms;
   }
 
@@ -1063,11 +1195,10 @@ struct Runner {
 
   void gather_all() {
     unsigned n = unsigned(progs.size());
-    dev::Params p = params();
-    CU(cudaMemcpyToSymbol(dev::g_P, &p, sizeof p));
+    const dev::Params p = params();
     d_gcount.alloc(n);
     unsigned blocks = (n + 127) / 128;
-    dev::gather_kernel<<<blocks, 128>>>(n, d_gcount.p, nullptr, nullptr);
+    dev::gather_kernel<<<blocks, 128>>>(p, n, d_gcount.p, nullptr, nullptr);
     CU(cudaGetLastError());
     gcount.resize(n);
     CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
@@ -1080,7 +1211,7 @@ struct Runner {
     d_goff.alloc(n);
     CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
     d_gpairs.alloc(2 * tot);
-    dev::gather_kernel<<<blocks, 128>>>(n, d_gcount.p, d_goff.p, d_gpairs.p);
+    dev::gather_kernel<<<blocks, 128>>>(p, n, d_gcount.p, d_goff.p, d_gpairs.p);
     CU(cudaGetLastError());
     gpairs.resize(2 * tot);
     if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
@@ -1154,6 +1285,7 @@ struct Server {
   DevBuf<DevInstr> d_instrs;
   DevBuf<dev::ull> d_labbits;
   DevBuf<dev::ServeReq> req;
+  DevBuf<dev::ull> spill;
   dev::ServeDone* done = nullptr;  // mapped host memory
   dev::ull* out = nullptr;         // mapped host memory
   dev::ServeReq* req_stage = nullptr;  // pinned staging for the async copies
@@ -1246,17 +1378,13 @@ struct Server {
     p.out = d_out;
     p.req_cap = req_cap;
     p.out_cap = out_cap;
-    CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, ks));
-    CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(dev::SMEM_BYTES)));
-    int bps = int(t.blocks_per_sm);
-    if (bps <= 0) {
-      int occ = 0;
-      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
-      bps = std::max(1, occ);
-    }
-    CU(cudaStreamSynchronize(ks));  // tables and parameters in place before the reducer starts
-    dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, ks>>>();
+    const unsigned grid = unsigned(sms * reducer_blocks_per_sm(t));
+    const uint64_t warps = uint64_t(grid) * dev::WARPS;
+    p.spill_cap = spill_cap_for(heap_bytes, warps);
+    spill.alloc(2 * size_t(p.spill_cap) * warps);
+    p.spill = spill.p;
+    CU(cudaStreamSynchronize(ks));  // tables in place before the reducer starts
+    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, ks>>>(p);
     CU(cudaGetLastError());
     running = true;
     slot_ticket.assign(nslots, 0);
@@ -1548,13 +1676,21 @@ namespace hvm {
 namespace noalloc {
 constexpr uint64_t SCRATCH_BYTES = uint64_t(64) << 20;  // 64 MiB in all
 constexpr unsigned QLOG2 = 12;                           // 4096 queue slots of 32 redexes
+// The reducer grid is capped at MAX_WARPS warps (4 blocks of 2 warps on
+// each of 148 SMs), each with an overflow stack of SPILL redexes, and lanes
+// take allocator chunks of CHUNK_NODES nodes: every lane holding a part-used
+// chunk ties up at most MAX_WARPS * 32 * CHUNK_NODES (303,104) nodes.
+constexpr unsigned MAX_WARPS = 148 * 4 * 2;
+constexpr unsigned SPILL = 256;
+constexpr unsigned CHUNK_NODES = 8;
 constexpr uint64_t round_up(uint64_t x) { return (x + 255) & ~uint64_t(255); }
 constexpr uint64_t OFF_CTRL = 0;
 constexpr uint64_t OFF_NET = round_up(OFF_CTRL + sizeof(dev::Ctrl));
 constexpr uint64_t OFF_QUEUE = round_up(OFF_NET + sizeof(dev::NetState));
 constexpr uint64_t OFF_BOOK = round_up(OFF_QUEUE + (uint64_t(1) << QLOG2) * sizeof(dev::Slot));
 constexpr uint64_t BOOK_BYTES = uint64_t(4) << 20;      // Def headers + instructions + label sets
-constexpr uint64_t OFF_HEAP = round_up(OFF_BOOK + BOOK_BYTES);
+constexpr uint64_t OFF_SPILL = round_up(OFF_BOOK + BOOK_BYTES);
+constexpr uint64_t OFF_HEAP = round_up(OFF_SPILL + uint64_t(MAX_WARPS) * SPILL * 16);
 constexpr uint64_t HEAP_BYTES = (SCRATCH_BYTES - OFF_HEAP) & ~uint64_t(15);
 static_assert(OFF_HEAP < SCRATCH_BYTES, "scratch layout");
 }  // namespace noalloc
@@ -1623,7 +1759,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   c.bump = 1;
   c.heap_nodes = HEAP_BYTES / 16;
   c.heap_bytes = HEAP_BYTES;
-  c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
+  c.chunk_nodes = t.chunk_nodes ? std::min<uint32_t>(t.chunk_nodes, 64) : CHUNK_NODES;
   c.spin_limit = 1ull << 24;
   c.donate_min = t.donate_min ? t.donate_min : 64;
   c.lane_budget = t.lane_budget ? t.lane_budget : 1;
@@ -1648,17 +1784,14 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   p.instrs = reinterpret_cast<const DevInstr*>(bk + off_ins);
   p.labbits = reinterpret_cast<const dev::ull*>(bk + off_lab);
   p.ndefs = unsigned(book.defs.size());
-  CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, st));
-  dev::boot_kernel<<<1, 128, 0, st>>>(0, 1);
+  p.spill = reinterpret_cast<dev::ull*>(base + OFF_SPILL);
+  p.spill_cap = SPILL;
+  hvm64_tuning tg = t;
+  if (tg.blocks_per_sm == 0 || tg.blocks_per_sm > 4) tg.blocks_per_sm = 4;
+  unsigned grid = std::min(unsigned(sms * reducer_blocks_per_sm(tg)), MAX_WARPS / unsigned(dev::WARPS));
+  dev::boot_kernel<<<1, dev::THREADS, dev::SMEM_BYTES, st>>>(p, 0, 1);
   CU(cudaGetLastError());
-  CU(cudaFuncSetAttribute(dev::reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dev::SMEM_BYTES)));
-  int bps = int(t.blocks_per_sm);
-  if (bps <= 0) {
-    int occ = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dev::reduce_kernel, dev::THREADS, dev::SMEM_BYTES));
-    bps = std::max(1, occ);
-  }
-  dev::reduce_kernel<<<unsigned(sms * bps), dev::THREADS, dev::SMEM_BYTES, st>>>();
+  dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>(p);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(st));
 

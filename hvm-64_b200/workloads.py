@@ -163,6 +163,34 @@ def church(k=5, last=2):
     return "\n".join(defs) + "\n"
 
 
+CHURCH_BIG_NORMAL_FORM = "(* (a a))"
+
+
+def church_big(nums=(2, 2, 2, 3)):
+    """The label-heavy Church net at 10^8-10^9 interactions.  Numerals with
+    one DUP label each (#1 .. #k) are applied to one another as in `church`:
+    n1 n2 n3 n4 = n4^(n3^(n2^n1)) = 3^16 for (2, 2, 2, 3).  Instead of the
+    eraser collapse (which discards almost all of the tower), the result is
+    forced the way tests/programs/stress_tests/boom.hvm forces its tower:
+    applied to `not` (@N = ((@F (@T a)) a)) and `true` (@T), so every one of
+    the 3^16 applications runs.  3^16 is odd: the normal form is `false`,
+    (* (a a)).  344,373,957 interactions (oracle)."""
+    def numeral(n, lab):
+        if n == 1:
+            return "((a R) (a R))"
+        fs = "(v1 v0)"
+        for i in range(1, n):
+            fs = f"#{lab}{{{fs} (v{i + 1} v{i})}}"
+        return f"({fs} (v{n} v0))"
+    defs = [f"@n{i + 1} = " + numeral(v, i + 1) for i, v in enumerate(nums)]
+    defs += ["@F = (* (x x))", "@T = (a (* a))", "@N = ((@F (@T a)) a)"]
+    arg = "(@N (@T R))"
+    for i in range(len(nums), 1, -1):
+        arg = f"(@n{i} {arg})"
+    defs.append(f"@main = R\n& @n1 ~ {arg}")
+    return "\n".join(defs) + "\n"
+
+
 def leaves(text):
     """Leaf values of a read-back Scott tree, left to right (Leaf x prints as
     `((x a) (* a))`, Node l r as `(* ((l' (r' b)) b))`)."""

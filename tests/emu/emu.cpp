@@ -64,14 +64,33 @@ void give(Emu* E, WarpSmem& W, unsigned& bot, unsigned cnt, int cur) {
   E->queue.push_back({unsigned(cur), std::move(v)});
 }
 
-void worker(Emu* E, unsigned share_min) {
+// One lane's share of work, like a reducer warp: a shared-memory stack plus
+// an overflow stack.  The stack a step may push into is kept tiny (`ring`
+// slots) so that pushes keep spilling into the overflow stack, whose own
+// small capacity sends the rest to the shared queue -- the paths a reducer
+// warp takes only under a burst of redexes.
+void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap) {
   g_emu = E;
   auto W = new_warp();
+  std::vector<ull> spill(2 * size_t(spill_cap) + 2);
+  W->sp = spill_cap ? spill.data() : nullptr;
+  W->sp_cap = spill_cap;
+  W->sp_n = 0;
   Ctx c{W.get(), 0, 0};
   unsigned top = 0, bot = 0;
   int cur = -1;
   for (;;) {
     if (ld_gpu32(&E->C.error)) break;
+    if (W->sp_n && top - bot < 4) {  // refill from the overflow stack's newest
+      unsigned m = std::min(W->sp_n, unsigned(SCAP - HEADROOM) - (top - bot));
+      for (unsigned i = 0; i < m; i++) {
+        unsigned k = (top + i) & (SCAP - 1);
+        W->stk[2 * k] = W->sp[2 * (W->sp_n - m + i)];
+        W->stk[2 * k + 1] = W->sp[2 * (W->sp_n - m + i) + 1];
+      }
+      top += m;
+      W->sp_n -= m;
+    }
     if (top == bot) {
       if (cur >= 0) {
         flush(*W, E->nets[cur]);
@@ -108,10 +127,14 @@ void worker(Emu* E, unsigned share_min) {
     top -= 1;
     W->ring_cnt = 0;
     W->ring_base = top;
-    W->ring_cap = unsigned(SCAP) - (top - bot);
+    W->ring_cap = std::min(unsigned(SCAP) - (top - bot), ring);
     interact(c, a, b);
     settle(c);
-    top += std::min(W->ring_cnt, unsigned(SCAP) - (top - bot));
+    {
+      unsigned cnt = W->ring_cnt;
+      top += std::min(cnt, W->ring_cap);
+      W->sp_n += spilled_of(W.get(), cnt);
+    }
     // merge reclaimed nodes into the pool
     int pn = std::max(W->pool_n, 0), fn = std::min(W->freed_n, POOL), mv = std::min(fn, POOL - pn);
     for (int k = 0; k < mv; k++) W->pool[pn + k] = W->freed[k];
@@ -121,13 +144,21 @@ void worker(Emu* E, unsigned share_min) {
     }
     W->pool_n = pn + mv;
     W->freed_n = 0;
-    if (top - bot >= share_min) {
+    if (top - bot + W->sp_n >= share_min) {
       bool want;
       {
         std::lock_guard<std::mutex> g(E->mu);
         want = E->queue.size() < 4;
       }
-      if (want) give(E, *W, bot, std::min(32u, (top - bot) / 2), cur);
+      if (want && W->sp_n >= 8) {  // the overflow stack's newest first
+        std::vector<ull> v(W->sp + 2 * (W->sp_n - 8), W->sp + 2 * W->sp_n);
+        W->sp_n -= 8;
+        atom_add(reinterpret_cast<ull*>(&E->nets[cur].pending), 1ull);
+        std::lock_guard<std::mutex> g(E->mu);
+        E->queue.push_back({unsigned(cur), std::move(v)});
+      } else if (want && top - bot >= 2) {
+        give(E, *W, bot, std::min(32u, (top - bot) / 2), cur);
+      }
     }
   }
   if (cur >= 0) flush(*W, E->nets[cur]);
@@ -142,9 +173,9 @@ void hvm::dev::push_overflow(unsigned net, ull a, ull b) {
   E->queue.push_back({net, std::vector<ull>{a, b}});
 }
 
-extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned threads, unsigned budget,
-                            unsigned share_min, uint64_t heap_bytes, uint64_t chunk, char** out_text, uint64_t* rw,
-                            char* err, size_t errcap) {
+extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned threads, unsigned ring,
+                            unsigned spill_cap, unsigned share_min, uint64_t heap_bytes, uint64_t chunk,
+                            char** out_text, uint64_t* rw, char* err, size_t errcap) {
   try {
     Book book;
     std::string src(book_text);
@@ -187,9 +218,8 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
       flush(*W, E.nets[0]);
       if (E.nets[0].pending > 0) E.C.nets_left = 1;
     }
-    (void)budget;
     std::vector<std::thread> th;
-    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min);
+    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min, std::max(1u, ring), spill_cap);
     for (auto& t : th) t.join();
     if (E.C.error) {
       snprintf(err, errcap, "device error %d info 0x%llx", E.C.error, (unsigned long long)E.C.error_info);

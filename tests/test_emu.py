@@ -25,17 +25,21 @@ def _lib():
                         *SRC, "-o", SO], check=True)
     L = ctypes.CDLL(SO)
     c = ctypes
-    L.hvm64emu_run.argtypes = [c.c_char_p, c.c_char_p, c.c_uint, c.c_uint, c.c_uint, c.c_uint64, c.c_uint64,
-                               c.POINTER(c.c_char_p), c.POINTER(c.c_uint64), c.c_char_p, c.c_size_t]
+    L.hvm64emu_run.argtypes = [c.c_char_p, c.c_char_p, c.c_uint, c.c_uint, c.c_uint, c.c_uint, c.c_uint64,
+                               c.c_uint64, c.POINTER(c.c_char_p), c.POINTER(c.c_uint64), c.c_char_p, c.c_size_t]
     return L
 
 
-def emu_run(text, threads=16, budget=4, heap=256 << 20, chunk=32):
+def emu_run(text, threads=16, ring=2, spill=24, heap=256 << 20, chunk=32):
+    """Reduce `text`'s @main on `threads` host threads.  A step may push into
+    at most `ring` stack slots; the rest go to a `spill`-redex overflow stack
+    and, past that, to the shared queue."""
     L = _lib()
     out = ctypes.c_char_p()
     rw = (ctypes.c_uint64 * 5)()
     err = ctypes.create_string_buffer(256)
-    rc = L.hvm64emu_run(text.encode(), b"main", threads, budget, 16, heap, chunk, ctypes.byref(out), rw, err, 256)
+    rc = L.hvm64emu_run(text.encode(), b"main", threads, ring, spill, 16, heap, chunk, ctypes.byref(out), rw,
+                        err, 256)
     assert rc == 0, err.value.decode()
     return out.value.decode(), dict(zip(("anni", "comm", "eras", "dref", "oper"), list(rw)))
 
@@ -71,3 +75,18 @@ def test_emu_deep_literal_def():
         text, rw = emu_run(src, threads=4)
         assert text == want
         assert rw == want_rw
+
+
+@pytest.mark.parametrize("ring,spill", [(2, 24), (512, 64), (512, 0)])
+def test_emu_radix_bursts(ring, spill):
+    """The radix-sort fixture at 2^9 keys: each @radix call pushes about 60
+    redexes at once, so the stack, the overflow stack and the shared queue
+    all take pushes; normal form and counts equal the oracle's."""
+    from oracle import oracle
+    src = next(p for p in PROGRAMS if p["name"] == "examples::sort::radix::radix_sort_ctr")["source"]
+    s = src.replace("& @gen ~ (20 (0 d))", "& @gen ~ (9 (0 d))")
+    assert s != src
+    want, want_rw, _ = oracle.run_book(s)
+    text, rw = emu_run(s, threads=16, ring=ring, spill=spill)
+    assert text == want
+    assert rw == want_rw

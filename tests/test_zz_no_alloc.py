@@ -18,10 +18,27 @@ def _hvm():
     return hvm64
 
 
+def _radix(keys_log2):
+    import json
+    import os
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "programs.json")
+    src = next(p for p in json.load(open(gold)) if p["name"] == "examples::sort::radix::radix_sort_ctr")["source"]
+    out = src.replace("& @gen ~ (20 (0 d))", f"& @gen ~ ({keys_log2} (0 d))")
+    assert out != src
+    return out
+
+
 CASES = [
     ("tree_sum_10", lambda: W.tree_sum(10, 4)),
     ("bitonic_8", lambda: W.bitonic(8, 5)),
     ("church_4", lambda: W.church(4)),
+    # wide nets: their work spreads over every warp of the grid, so every
+    # lane's allocator chunk is taken at once
+    ("tree_sum_16", lambda: W.tree_sum(16, 6)),
+    ("bitonic_12", lambda: W.bitonic(12, 7)),
+    # Def calls that push about 60 redexes each: the warps' overflow stacks
+    # and the queue take the bursts
+    ("radix_2^12", lambda: _radix(12)),
 ]
 
 
@@ -71,8 +88,8 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
         hvm64.normal_noalloc(big, "main")
     assert e.value.code == hvm64.ERR_BAD_INPUT and "too large" in str(e.value)
     # a net that outgrows the built-in heap (a generated tree of 2^22 leaves,
-    # kept whole: far more than its 3.7 million nodes) stops with OOM, and the
-    # next call works
+    # kept whole: far more than its 3.49 million nodes) stops with OOM, and
+    # the next call works
     gen_only = W.tree_sum(22, 0).replace("@main = a\n& @sum ~ (b a)\n& @gen ~ (22 (0 b))",
                                          "@main = a\n& @gen ~ (22 (0 a))")
     assert "& @gen ~ (22 (0 a))" in gen_only
