@@ -1,25 +1,32 @@
 #!/usr/bin/env python
 """Benchmark: batched HVM-64 net normalisation on B200.
 
-Workload (one step): a batch of independent nets (default 4096), each a
-tree-sum or a bitonic sort chosen 50/50 by seed, depth drawn log-uniform in
-[dmin, dmax], reduced to normal form in ONE persistent launch through the C
-ABI (include/hvm64.h).  Metric: interactions (ANNI+COMM+ERAS+DREF+OPER, the
+Workload: the batched configuration -- 4096 independent nets, each a tree-sum
+or a bitonic sort chosen 50/50 by seed, depth drawn log-uniform in [8, 18]
+(u24 keys from an in-net mixer), reduced to normal form through the C ABI
+(include/hvm64.h).  Metric: interactions (ANNI+COMM+ERAS+DREF+OPER, the
 reference's Rewrites::total) per second, in G/s.
+
+Steps.  The batch is split into K size-balanced slices (longest-processing-
+time on the predicted interaction count), K = --steps; step k reduces slice k
+in ONE persistent launch (boot + reduce, replayed as a captured CUDA graph).
+The K timed steps therefore reduce every net of the batch exactly once, and
+`value` is the whole batch's interactions over the K steps' device time.
+Warm-up steps reduce the first W slices first.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun the job reduces nets x N nets, split over the ranks by a
-size-balanced partition (weak scaling: each GPU keeps about `nets` nets); no
-collective on the data path (the nets are independent), only the step time
-(max over ranks) and the interaction count (sum) are reduced.
+Under torchrun each rank takes a size-balanced share of a global batch of
+nets x N nets (weak scaling); nothing crosses ranks while they reduce, only
+the step time (max over ranks) and the interaction count (sum).
 `--impl reference` times the CPU evaluator (the oracle's restatement of the
 reference's Net::parallel_normal; the Rust reference cannot be built without
-a Rust toolchain) on a bounded sample of the same workload.
+a Rust toolchain) on mass-weighted samples of the same batch.
 """
 import argparse
 import json
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -30,6 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hvm-64_b200"))
 
 import workloads as W  # noqa: E402
+import shard  # noqa: E402
 
 METRIC = "GInteractions/s on 1 B200, batched-persistent vs per-net plain; p99 latency"
 UNIT = "GInteractions/s"
@@ -37,13 +45,9 @@ UNIT = "GInteractions/s"
 # Algorithmic bytes per interaction (HBM model: one port word = 8 B, an
 # exchange or CAS counts a read and a write).
 BYTES = {"anni": 224, "comm22": 384, "comm02": 128, "eras": 0, "oper": 104}
-
-# DRAM bytes (read + write) per interaction of reduce_kernel: ncu's
-# dram__bytes_read.sum + dram__bytes_write.sum (68.06 + 151.11 GB) over the
-# 1,414,382,623 interactions of one launch on a 4096-net batch of depth [8, 9]
-# (the full workload is too long to capture); scaled by the interactions of a
-# launch.
-TRAFFIC_PER_INTERACTION = (68.06e9 + 151.11e9) / 1414382623
+# Global atomics per interaction of the same model (exchange or CAS); a Def
+# call takes about one per link to its argument.
+ATOMICS = {"anni": 8, "comm22": 8, "comm02": 4, "oper": 2}
 
 
 def dref_bytes(nodes, links, calls):
@@ -57,11 +61,6 @@ def algorithmic_bytes(counts, stats):
             counts["oper"] * BYTES["oper"] + dref_bytes(stats["dref_nodes"], stats["dref_links"], counts["dref"]))
 
 
-# Global atomics per interaction of the same model (exchange or CAS); a Def
-# call takes about one per link to its argument.
-ATOMICS = {"anni": 8, "comm22": 8, "comm02": 4, "oper": 2}
-
-
 def algorithmic_atomics(counts, stats):
     comm22 = stats["comm22"]
     comm02 = counts["comm"] - comm22
@@ -69,14 +68,30 @@ def algorithmic_atomics(counts, stats):
             counts["oper"] * ATOMICS["oper"] + stats["dref_links"])
 
 
-def atomic_peak():
-    """The measured L2 atomic rate (ops/s), if the microbenchmark's line was
-    saved beside the measured peaks; else None."""
+def _profile(name):
     try:
-        p = json.load(open(os.path.join(ROOT, "profiles", "atomic_peak.json")))
-        return min(float(p["atomic_exch_gops"]), float(p["atomic_cas_gops"])) * 1e9
+        return json.load(open(os.path.join(ROOT, "profiles", name)))
     except Exception:
         return None
+
+
+def atomic_peak():
+    """The measured L2 atomic rate (ops/s) of 64-bit exchange and CAS on random
+    words (profiles/atomic_peak.json, hvm64_atomic_peak); else None."""
+    p = _profile("atomic_peak.json")
+    if not p:
+        return None, None
+    r = p.get("rate_for_roofline") or p
+    return min(float(r["atomic_exch_gops"]), float(r["atomic_cas_gops"])) * 1e9, p.get("note")
+
+
+def traffic_per_interaction():
+    """DRAM bytes (read + write) per interaction of reduce_kernel from the
+    current build's ncu capture summarised in profiles/ (None if absent)."""
+    p = _profile("reduce_kernel_traffic.json")
+    if not p:
+        return None, None
+    return float(p["dram_bytes_per_interaction"]), p.get("capture")
 
 
 def peaks():
@@ -147,25 +162,57 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline(entries, budget, threads):
-    """The oracle's parallel evaluator on the first nets of the batch whose
-    estimated interactions fit `budget`; returns (interactions/s, sample)."""
-    from oracle import oracle
-    sample, est = [], 0.0
-    for e in entries:
-        c = W.est_interactions(e[0], e[1])
-        if sample and est + c > budget:
+def est(e):
+    return W.est_interactions(e[0], e[1])
+
+
+def slices_of(entries, k):
+    """The batch split into k size-balanced slices (lists of entries)."""
+    parts = shard.lpt_partition([est(e) for e in entries], k)
+    return [[entries[i] for i in p] for p in parts]
+
+
+def mass_sample(entries, budget, seed, first_may_exceed=True):
+    """Nets drawn with probability proportional to their predicted
+    interactions (without replacement) until `budget` interactions: the
+    sample's size distribution follows the batch's interaction mass, so big
+    nets are represented as they weigh in the batch's time."""
+    rng = random.Random(seed)
+    pool = list(entries)
+    out, tot = [], 0.0
+    while pool and tot < budget:
+        w = [est(e) for e in pool]
+        e = rng.choices(pool, weights=w)[0]
+        pool.remove(e)
+        c = est(e)
+        if out and tot + c > budget:
             continue
-        sample.append(e)
-        est += c
+        if not out and c > budget and not first_may_exceed:
+            continue
+        out.append(e)
+        tot += c
+    return out
+
+
+def cpu_run(sample, threads):
+    """The oracle's parallel evaluator on each sampled net: (interactions,
+    seconds inside normal, description)."""
+    from oracle import oracle
     text = W.batch_book(sample)
     total, secs = 0, 0.0
     for kind, d, j in sample:
         _, rw, s = oracle.run_book(text, entry=f"main_{j}", mode=oracle.MODE_PARALLEL, threads=threads)
         total += sum(rw.values())
         secs += s
-    desc = (f"{len(sample)} of the batch's nets ({total} interactions): the C++ restatement of "
-            f"Net::parallel_normal, {threads} threads, timer around normal only")
+    depths = sorted(f"{k}{d}" for k, d, _ in sample)
+    desc = (f"{len(sample)} nets drawn from the batch with probability proportional to their size "
+            f"({', '.join(depths)}; {total} interactions): the C++ restatement of Net::parallel_normal, "
+            f"{threads} threads, timer around normal only")
+    return total, secs, desc
+
+
+def cpu_baseline(entries, budget, threads, seed=0):
+    total, secs, desc = cpu_run(mass_sample(entries, budget, seed), threads)
     return total / secs / 1e9, desc
 
 
@@ -182,7 +229,6 @@ def serve_leg(args, hvm64):
     (tree-sum / bitonic sort / Church, sizes log-uniform 1e3..1e8
     interactions) served by the continuous-batching server, against the plain
     path that reduces one request per launch, first come first served."""
-    import random
     reqs = W.serving_requests(args.serve_requests, seed=0)
     book = hvm64.Book.from_str(W.serving_book(reqs))
     names = [f"main_{j}" for _, _, j in reqs]
@@ -216,9 +262,11 @@ def serve_leg(args, hvm64):
             start = max(a, free_at)
             free_at = start + sv_s
             lat_plain.append(free_at - a)
-        # continuous batching, in real time
+        # continuous batching, in real time; the server's lifetime ends soon
+        # after the last arrival's wait, so closing it never blocks long
+        life_ms = int(1000 * (arr[-1] + args.serve_wait_s)) + 5000
         sv = hvm64.Server(book, slots=args.serve_slots, out_pairs=1 << 18, heap_bytes=16 << 30,
-                          tuning=hvm64.Tuning(timeout_ms=600000))
+                          tuning=hvm64.Tuning(timeout_ms=life_ms))
         lat, owner, inflight, i = [], {}, 0, 0
         t_start = time.perf_counter()
         last = 0.0
@@ -261,10 +309,12 @@ def serve_leg(args, hvm64):
                     "requests is close to the maximum"}
 
 
-def config(args):
+def config(args, k):
     return {"workload": f"batched {args.nets} nets: tree-sum / bitonic-sort 50-50 by seed, depth log-uniform "
                         f"[{args.dmin}, {args.dmax}], u24 keys",
-            "nets": args.nets, "dmin": args.dmin, "dmax": args.dmax, "mode": "persistent, one launch per step",
+            "nets": args.nets, "dmin": args.dmin, "dmax": args.dmax,
+            "steps_cover": f"the batch split into {k} size-balanced slices, one persistent launch (CUDA graph) "
+                           f"per slice; the {k} timed steps reduce every net once",
             "l2": "flushed between steps (512 MiB write); heaps far above L2",
             "parallelism": f"weak: {args.gpus} x 1 GPU, size-balanced disjoint shares of nets x {args.gpus} nets"}
 
@@ -274,43 +324,93 @@ def run_reference(args):
         return
     t, n = pow2_threads()
     entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=0)
-    vals = []
+    k = max(1, args.steps)
+    vals, descs = [], []
     for step in range(args.warmup + args.steps):
-        v, desc = cpu_baseline(entries, args.cpu_budget / 4, t)
+        sample = mass_sample(entries, args.ref_budget, seed=1000 + step)
+        total, secs, desc = cpu_run(sample, t)
         if step >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+            vals.append((total, secs))
+            descs.append(desc)
+    value = sum(a for a, _ in vals) / sum(b for _, b in vals) / 1e9
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": t, "kind": "port", "sample": desc,
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args, k),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": t, "kind": "port",
+                         "sample": f"per step: {descs[0] if descs else ''} (a fresh mass-weighted draw per step; "
+                                   f"value = all timed steps' interactions over their normal() time)",
                          "host_cpus": n},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
 
 
+def single_net_leg(hvm64, args, hbm):
+    """The single-net bitonic sort of 2^20 keys (8.8e9 interactions): device
+    throughput and its own roofline record, checked against the golden
+    counts."""
+    text = W.bitonic(args.single_depth, 2)
+    book = hvm64.Book.from_str(text)
+    net = hvm64.Net(book, int(args.single_heap_gb * (1 << 30)))
+    tune = hvm64.Tuning(timeout_ms=600000)
+    net.boot("main")
+    rw = net.normal(tune)
+    ms = net.device_ms
+    st = net.stats()
+    counts = rw.as_dict()
+    got = net.readback()
+    ok = W.leaves(got) == sorted(W.sort_keys(args.single_depth, 2))
+    gold = None
+    try:
+        gold = json.load(open(os.path.join(ROOT, "tests", "golden", "workload_counts.json")))[
+            f"bitonic_{args.single_depth}_2"]["counts"]
+    except Exception:
+        pass
+    alg = algorithmic_bytes(counts, st)
+    atoms = algorithmic_atomics(counts, st)
+    arate, _ = atomic_peak()
+    ach = alg / (ms / 1000.0) / 1e9
+    tpi, _ = traffic_per_interaction()
+    del net
+    return {"workload": f"single net: bitonic sort of 2^{args.single_depth} u24 keys (seed 2)",
+            "value": rw.total() / (ms / 1000.0) / 1e9, "unit": UNIT, "device_ms": ms,
+            "interactions": rw.total(), "sorted": ok, "counts_match_golden": (counts == gold) if gold else None,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "traffic": tpi * rw.total() if tpi else None, "algorithmic_bytes": alg,
+                         "algorithmic_atomics": atoms,
+                         "atomic_frac": (atoms / (ms / 1000.0)) / arate if arate else None,
+                         "frac_of_bound": max(ach / hbm, (atoms / (ms / 1000.0)) / arate if arate else 0)},
+            "heap_nodes_used": st["heap_nodes_used"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nets", type=int, default=4096)
     ap.add_argument("--dmin", type=int, default=8)
-    ap.add_argument("--dmax", type=int, default=14)
+    ap.add_argument("--dmax", type=int, default=18)
     ap.add_argument("--plain-nets", type=int, default=256, help="nets timed one-per-launch for the plain arm")
-    ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-budget", type=float, default=4e8, help="interactions in the CPU sample")
-    ap.add_argument("--heap-gb", type=float, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2, help="slices timed end to end through the public API")
+    ap.add_argument("--cpu-budget", type=float, default=2e9, help="interactions in the CPU-baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=5e8, help="interactions per reference-arm step")
+    ap.add_argument("--count-check", type=float, default=3e8,
+                    help="interactions of the nets whose per-rule counts are checked against the oracle")
+    ap.add_argument("--heap-gb", type=float, default=48)
     ap.add_argument("--device-only", action="store_true", help="skip the plain, e2e, serving and CPU legs")
     ap.add_argument("--serve-requests", type=int, default=96, help="requests per offered load (0: no serving leg)")
     ap.add_argument("--serve-slots", type=int, default=64)
     ap.add_argument("--serve-wait-s", type=float, default=120.0,
                     help="give up on a load this long after its last arrival")
+    ap.add_argument("--single-depth", type=int, default=20, help="single-net bitonic leg: 2^d keys (0: skip)")
+    ap.add_argument("--single-heap-gb", type=float, default=32)
+    ap.add_argument("--full-launch", action="store_true",
+                    help="also time all nets in ONE launch (one step of the whole batch)")
     ap.add_argument("--autotune", type=int, default=1, help="pick the launch knobs on a sample first (0: defaults)")
-    ap.add_argument("--tune-sample", type=int, default=1024)
+    ap.add_argument("--tune-budget", type=float, default=3e9, help="interactions in the autotuner's sample")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -332,95 +432,137 @@ def main():
     if world > 1:
         # one global batch of nets x world nets, split into size-balanced
         # shares (no communication while they reduce)
-        import shard
         glob = W.batch_entries(args.nets * world, args.dmin, args.dmax, seed=0)
-        entries = shard.rank_share(glob, lambda e: W.est_interactions(e[0], e[1]), rank, world)
+        entries = shard.rank_share(glob, est, rank, world)
     else:
         entries = W.batch_entries(args.nets, args.dmin, args.dmax, seed=0)
-    text = W.batch_book(entries)
+    K = max(1, args.steps)
+    slices = slices_of(entries, K)
+    order = [e for s in slices for e in s]  # the Batch holds the nets slice by slice
+    bounds, o = [], 0
+    for s in slices:
+        bounds.append((o, len(s)))
+        o += len(s)
+    text = W.batch_book(order)
     book = hvm64.Book.from_str(text)
-    names = [f"main_{j}" for _, _, j in entries]
+    names = [f"main_{j}" for _, _, j in order]
     heap = int(args.heap_gb * (1 << 30))
     tune_report = None
     if args.autotune:
         import autotune
-        tune, tune_report = autotune.autotune(book, names, heap, sample=args.tune_sample, timeout_ms=600000)
+        sample = mass_sample(entries, args.tune_budget, seed=7, first_may_exceed=False)
+        tune, tune_report = autotune.autotune(book, [f"main_{j}" for _, _, j in sample], heap,
+                                              sample=len(sample), timeout_ms=600000)
     else:
         tune = hvm64.Tuning(timeout_ms=600000)
-    tune.flags |= hvm64.TUNE_GRAPH  # each step replays one captured CUDA graph
+    tune.flags |= hvm64.TUNE_GRAPH  # each step replays a captured CUDA graph
     batch = hvm64.Batch(book, names, heap)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
-    for _ in range(args.warmup):
-        batch.normal(hvm64.PERSISTENT, tune)
-    # every net's normal form, checked outside the timed region
-    bad = sum(0 if W.check_result(kind, d, j, batch.readback(i)) else 1 for i, (kind, d, j) in enumerate(entries))
-    total_per_step = sum(batch.rwts[i].total() for i in range(batch.n))
-    counts = {k: sum(getattr(batch.rwts[i], k) for i in range(batch.n))
-              for k in ("anni", "comm", "eras", "dref", "oper")}
+    def check_slice(k):
+        f, c = bounds[k]
+        bad = 0
+        for i in range(f, f + c):
+            kind, d, j = order[i]
+            bad += 0 if W.check_result(kind, d, j, batch.readback(i)) else 1
+        return bad
+
+    for w in range(args.warmup):
+        f, c = bounds[w % K]
+        batch.normal(hvm64.PERSISTENT, tune, first=f, count=c)
 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms, kernel_ms = [], []
+    step_ms, kernel_ms, bad = [], [], 0
+    agg_stats = {}
     with Clocks(local) as clk:
-        for _ in range(args.steps):
+        for k in range(K):
+            f, c = bounds[k]
             flush.fill_(1)
+            torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            batch.normal(hvm64.PERSISTENT, tune)
+            batch.normal(hvm64.PERSISTENT, tune, first=f, count=c)
             e1.record()
             torch.cuda.synchronize()
             step_ms.append(e0.elapsed_time(e1))
             kernel_ms.append(batch.device_ms)
+            st = batch.stats()
+            for key, v in st.items():
+                agg_stats[key] = agg_stats.get(key, 0) + v
+            bad += check_slice(k)  # every net's normal form, outside the step's events
     torch.cuda.synchronize()
     elapsed = sum(step_ms) / 1000.0
-    stats = batch.stats()
+    total_per_rank = sum(batch.rwts[i].total() for i in range(batch.n))
+    counts = {key: sum(getattr(batch.rwts[i], key) for i in range(batch.n))
+              for key in ("anni", "comm", "eras", "dref", "oper")}
     if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-        tot = torch.tensor([float(total_per_step)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tot)
-        total_all = float(tot.item())
+        elapsed = shard.max_over_ranks(elapsed, dist, "cuda")
+        total_all = shard.sum_over_ranks(total_per_rank, dist, "cuda")
     else:
-        total_all = float(total_per_step)
-    value = total_all * args.steps / elapsed / 1e9
+        total_all = float(total_per_rank)
+    value = total_all / elapsed / 1e9
 
-    # roofline of reduce_kernel: algorithmic bytes of one launch over its
-    # device time (CUDA events the library records on its launching stream)
+    # per-rule counts of a mass-weighted sample of nets against the oracle
+    count_check = None
+    if rank == 0 and not args.device_only and args.count_check > 0:
+        from oracle import oracle
+        t, _ = pow2_threads()
+        sample = mass_sample(entries, args.count_check, seed=11, first_may_exceed=False)
+        idx = {e: i for i, e in enumerate(order)}
+        mism = 0
+        for e in sample:
+            _, want, _ = oracle.run_book(text, entry=f"main_{e[2]}", mode=oracle.MODE_PARALLEL, threads=t)
+            mism += 0 if batch.rwts[idx[e]].as_dict() == want else 1
+        count_check = {"nets": len(sample), "interactions": int(sum(est(e) for e in sample)),
+                       "mismatches": mism, "sample": "mass-weighted draw of nets up to the budget"}
+
+    # roofline of reduce_kernel: algorithmic bytes of the timed launches over
+    # their device time (CUDA events the library records on its stream)
     hbm, peak_kind = peaks()
-    alg = algorithmic_bytes(counts, stats)
-    atoms = algorithmic_atomics(counts, stats)
-    arate = atomic_peak()
-    kms = statistics.mean(kernel_ms)
-    achieved = alg / (kms / 1000.0) / 1e9
-    traffic = TRAFFIC_PER_INTERACTION * total_per_step if TRAFFIC_PER_INTERACTION else None
+    alg = algorithmic_bytes(counts, agg_stats)
+    atoms = algorithmic_atomics(counts, agg_stats)
+    arate, anote = atomic_peak()
+    ksec = sum(kernel_ms) / 1000.0
+    achieved = alg / ksec / 1e9
+    tpi, tcap = traffic_per_interaction()
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args),
-        "interactions_per_step": total_per_step, "counts_per_step": counts, "nets_bad": bad,
+        "warmup": args.warmup, "ms_per_step": elapsed * 1000.0 / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config(args, K),
+        "interactions": total_all, "counts": counts, "nets_bad": bad, "count_check": count_check,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",
-                     "kernel": "reduce_kernel (+ boot_kernel) device time per launch", "kernel_ms": kms,
-                     "algorithmic_bytes": alg, "algorithmic_atomics": atoms,
-                     "atomic_rate_ops": arate,
-                     "atomic_frac": (atoms / (kms / 1000.0)) / arate if arate else None},
-        "gpu_launches": 4 * args.steps,
-        "tuning": {"knobs": {k: getattr(tune, k) for k in ("blocks_per_sm", "chunk_nodes", "donate_min",
-                                                            "queue_slots_log2")},
+                     "traffic": tpi * total_per_rank / K if tpi else None,
+                     "traffic_source": tcap, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                     "kernel": "reduce_kernel (+ boot_kernel) device time per launch (one launch per step)",
+                     "kernel_ms_per_launch": 1000.0 * ksec / K,
+                     "algorithmic_bytes_per_launch": alg / K, "algorithmic_atomics_per_launch": atoms / K,
+                     "atomic_rate_ops": arate, "atomic_rate_note": anote,
+                     "atomic_frac": (atoms / ksec) / arate if arate else None},
+        "gpu_launches": 4 * K,
+        "tuning": {"knobs": {key: getattr(tune, key) for key in ("blocks_per_sm", "chunk_nodes", "donate_min",
+                                                                  "queue_slots_log2")},
                    "cuda_graph": True, "autotune": tune_report},
         "clocks": clk.summary(),
-        "device_stats": stats,
+        "device_stats": agg_stats,
     }
+
+    if args.full_launch:
+        # the whole batch in ONE persistent launch (no slicing)
+        batch.normal(hvm64.PERSISTENT, tune)
+        fl = batch.device_ms
+        tot = sum(batch.rwts[i].total() for i in range(batch.n))
+        out["full_launch"] = {"value": tot / (fl / 1000.0) / 1e9, "unit": UNIT, "device_ms": fl,
+                              "interactions": tot, "nets": batch.n}
 
     if not args.device_only:
         # plain arm: the batch's first `plain_nets` nets, one launch each
         plain_entries = entries[:args.plain_nets]
         if plain_entries:
-            pbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
+            pnames = [f"main_{j}" for _, _, j in plain_entries]
+            pbatch = hvm64.Batch(book, pnames, heap)
             ptune = hvm64.Tuning(timeout_ms=600000)
             pbatch.normal(hvm64.PLAIN, ptune)
             ptotal = sum(pbatch.rwts[i].total() for i in range(pbatch.n))
@@ -431,7 +573,7 @@ def main():
             pdev = pbatch.device_ms
             del pbatch
             # the batched reducer on the same subset, for the like-for-like ratio
-            sbatch = hvm64.Batch(book, names[:len(plain_entries)], heap)
+            sbatch = hvm64.Batch(book, pnames, heap)
             sbatch.normal(hvm64.PERSISTENT, tune)
             s0 = time.perf_counter()
             sbatch.normal(hvm64.PERSISTENT, tune)
@@ -441,38 +583,46 @@ def main():
                             "device_value": ptotal / (pdev / 1000.0) / 1e9,
                             "batched_same_nets": ptotal / sub_s / 1e9,
                             "note": "one net per launch (wall time incl. launch + sync) vs the batched "
-                                    "reducer on the same nets, and the full batch's value"}
+                                    "reducer on the same nets in one launch"}
 
-        # e2e through the public API from host memory: tables and net list to
+        # e2e through the public API from host memory, per slice: net list to
         # the device, reduce, every net's normal form back to host text.
-        e2e_s, h2d, d2h = 0.0, 0, 0
-        for _ in range(args.e2e_steps):
+        e2e_s, e2e_tot, h2d, d2h = 0.0, 0, 0, 0
+        ne = max(1, min(args.e2e_steps, K))
+        for k in range(ne):
+            f, c = bounds[k]
             torch.cuda.synchronize()
             e0 = time.perf_counter()
-            ebatch = hvm64.Batch(book, names, heap)
+            ebatch = hvm64.Batch(book, names[f:f + c], heap)
             ebatch.normal(hvm64.PERSISTENT, tune)
             for i in range(ebatch.n):
                 ebatch.readback(i)
             e2e_s += time.perf_counter() - e0
+            e2e_tot += sum(ebatch.rwts[i].total() for i in range(ebatch.n))
             st = ebatch.stats()
-            h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+            h2d += st["h2d_bytes"]
+            d2h += st["d2h_bytes"]
             del ebatch
         if dist:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        out["e2e"] = {"value": total_all * args.e2e_steps / e2e_s / 1e9, "unit": UNIT,
-                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                      "note": "Batch create + normal + readback of every net, wall clock"}
-
-        if rank == 0 and args.serve_requests > 0:
-            del batch
-            try:
-                out["serving"] = serve_leg(args, hvm64)
-            except Exception as e:  # the serving leg must not cost the benchmark line
-                out["serving"] = {"error": f"{type(e).__name__}: {e}"}
+            e2e_s = shard.max_over_ranks(e2e_s, dist, "cuda")
+        out["e2e"] = {"value": e2e_tot * (world if dist else 1) / e2e_s / 1e9, "unit": UNIT,
+                      "h2d_bytes_per_step": h2d // ne, "d2h_bytes_per_step": d2h // ne,
+                      "steps": ne,
+                      "note": "per slice: Batch create (Book tables + net list to the device) + normal + "
+                              "readback of every net's normal form to host text, wall clock"}
 
         if rank == 0:
+            del batch
+            if args.single_depth:
+                try:
+                    out["single_net"] = single_net_leg(hvm64, args, hbm)
+                except Exception as e:
+                    out["single_net"] = {"error": f"{type(e).__name__}: {e}"}
+            if args.serve_requests > 0:
+                try:
+                    out["serving"] = serve_leg(args, hvm64)
+                except Exception as e:  # the serving leg must not cost the benchmark line
+                    out["serving"] = {"error": f"{type(e).__name__}: {e}"}
             t, n = pow2_threads()
             try:
                 v, desc = cpu_baseline(entries, args.cpu_budget, t)

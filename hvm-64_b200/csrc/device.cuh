@@ -34,10 +34,18 @@ namespace dev {
 
 typedef unsigned long long ull;
 
+#ifndef HVM_SCAP
+#define HVM_SCAP 512
+#endif
+#ifndef HVM_HEADROOM
+#define HVM_HEADROOM 192
+#endif
 constexpr int WARPS = 2;            // warps per reducer block
 constexpr int THREADS = WARPS * 32;
-constexpr int SCAP = 512;           // per-warp shared-memory redex stack (power of two)
-constexpr int HEADROOM = 192;       // stack slots kept free for the redexes of one step
+constexpr int SCAP = HVM_SCAP;      // per-warp shared-memory redex stack (power of two)
+constexpr int HEADROOM = HVM_HEADROOM;  // stack slots kept free for the redexes of one step
+static_assert((SCAP & (SCAP - 1)) == 0 && SCAP >= 64, "SCAP is a power of two, at least 64");
+static_assert(HEADROOM >= 0 && SCAP - HEADROOM >= 32, "a step's window needs SCAP - HEADROOM >= 32");
 constexpr int CHUNK = 32;           // redexes per global-queue slot
 constexpr int POOL = 64;            // per-warp pool of free nodes ready for reuse
 constexpr unsigned ICACHE = 32;     // instructions of the step's Def staged in shared memory

@@ -34,13 +34,15 @@ namespace dev {
 
 // ---- global redex queue --------------------------------------------------------
 // Single-thread reservation; data movement may be done by the whole warp.
-// Never waits for a consumer: a full queue (or a reservation that keeps
-// losing its CAS) returns false and the caller keeps the work.
+// Never waits for a consumer: a full queue returns false at once and the
+// caller keeps the work.  A lost CAS means another producer got its slot, so
+// retrying under contention always makes progress; the retry count is still
+// bounded (then the reservation fails like a full queue).
 __device__ bool q_reserve_push(ull& pos) {
   Ctrl* C = g_P.ctrl;
   ull mask = C->q_mask;
   pos = ld_gpu(&C->q_tail);
-  for (int tries = 0; tries < 256; tries++) {
+  for (unsigned tries = 0; tries < (1u << 20); tries++) {
     Slot* s = &g_P.q[pos & mask];
     long long dif = (long long)ld_gpu(&s->seq) - (long long)pos;
     if (dif == 0) {
@@ -48,10 +50,11 @@ __device__ bool q_reserve_push(ull& pos) {
       if (old == pos) return true;
       pos = old;
     } else if (dif < 0) {
-      return false;  // full
+      return false;  // full: the slot still holds the previous lap's redexes
     } else {
       pos = ld_gpu(&C->q_tail);
     }
+    if ((tries & 63) == 63 && run_failed()) return false;
   }
   return false;
 }
@@ -90,7 +93,7 @@ __device__ void q_release(ull pos) {
 __device__ __noinline__ void push_overflow(unsigned net, ull a, ull b) {
   ull pos;
   if (!q_reserve_push(pos)) {
-    run_fail(net, HVM64_ERR_QUEUE, 0);
+    run_fail(net, HVM64_ERR_QUEUE, 1);
     return;
   }
   atomicAdd(reinterpret_cast<ull*>(&g_P.nets[net].pending), 1ull);
@@ -199,11 +202,12 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
 // or writes its net's pairs at offs[i].  A net whose walk overflows the
 // stack gets count ~0u and is read back from a heap image instead.
 constexpr unsigned GATHER_STACK = 256;
-__global__ void gather_kernel(const __grid_constant__ Params P, unsigned n, unsigned* counts, const ull* offs,
-                              ull* out) {
+__global__ void gather_kernel(const __grid_constant__ Params P, unsigned first, unsigned n, unsigned* counts,
+                              const ull* offs, ull* out) {
   load_params(P);
   unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  i += first;
   ull stk[GATHER_STACK];
   bool deep = false;
   ull root = g_P.nets[i].root;
@@ -290,10 +294,13 @@ __device__ __noinline__ unsigned serve_admit(WarpSmem& W, Ctx& c) {
 #endif
 constexpr int QW = HVM_QW;  // selection window: 32 * QW newest redexes
 
+#ifndef HVM_MINB
+#define HVM_MINB 7
+#endif
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
-__global__ void __launch_bounds__(THREADS, 7) reduce_kernel(const __grid_constant__ Params P) {
+__global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_constant__ Params P) {
   load_params(P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
@@ -344,7 +351,8 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel(const __grid_constan
     // steps stay full and the warp keeps the net while either holds work.
     {
       const unsigned spn = W.sp_n;
-      if (spn && top - bot < 64u) {
+      constexpr unsigned LOW = unsigned(SCAP - HEADROOM) < 64u ? unsigned(SCAP - HEADROOM) : 64u;
+      if (spn && top - bot < LOW) {
         unsigned m = min(spn, unsigned(SCAP - HEADROOM) - (top - bot));
         const ull* src = W.sp + 2ull * (spn - m);
         for (unsigned i = lane; i < m; i += 32) {
@@ -645,23 +653,26 @@ __global__ void __launch_bounds__(THREADS, 7) reduce_kernel(const __grid_constan
       __syncwarp();
     }
 
-    // Share work when other warps are starving: the overflow stack first,
-    // then the oldest half of the shared-memory stack (at most four slots
-    // per check).
-    if (top - bot + W.sp_n >= unsigned(C->donate_min) && ((step & 7) == 0)) {
+    // Share work when other warps are starving, and move work to the global
+    // queue when the overflow stack is three quarters full: the overflow
+    // stack first, then the oldest half of the shared-memory stack (at most
+    // four slots per check).
+    const bool sp_high = W.sp_n > W.sp_cap - W.sp_cap / 4u;
+    if (top - bot + W.sp_n >= unsigned(C->donate_min) && ((step & 7) == 0 || sp_high)) {
       int give = 0;
       if (lane == 0) {
         long long h = ld_gpu64s(&C->hungry);
         long long queued = (long long)(ld_gpu(&C->q_tail) - ld_gpu(&C->q_head));
-        give = h > 0 && queued < h;
+        give = (h > 0 && queued < h) ? 2 : sp_high ? 1 : 0;
       }
-      if (__shfl_sync(0xffffffffu, give, 0)) {
+      give = __shfl_sync(0xffffffffu, give, 0);
+      if (give) {
         unsigned k = 0;
         for (; k < 4u && W.sp_n >= 32u; k++) {
           if (!donate_spill(W, cur)) break;
           if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
         }
-        for (unsigned chunks = min((top - bot) / 64u, 4u - k); chunks; chunks--) {
+        for (unsigned chunks = give == 2 ? min((top - bot) / 64u, 4u - k) : 0u; chunks; chunks--) {
           if (!donate(S, bot, 32u, cur)) break;
           if (lane == 0) atomicAdd(&C->stat_donated, 1ull);
         }
@@ -728,7 +739,7 @@ __global__ void __launch_bounds__(THREADS) boot_kernel(const __grid_constant__ P
       unsigned k = min(total - done, unsigned(CHUNK));
       ull ra = lane < k ? W.stk[2 * (done + lane)] : 0, rb = lane < k ? W.stk[2 * (done + lane) + 1] : 0;
       if (!donate_vals(ra, rb, k, int(i))) {
-        if (lane == 0) run_fail(i, HVM64_ERR_QUEUE, 0);
+        if (lane == 0) run_fail(i, HVM64_ERR_QUEUE, 2);
         break;
       }
     }
@@ -946,9 +957,18 @@ struct Runner {
     CU(cudaMemcpyAsync(ctrl.p, &c, sizeof c, cudaMemcpyHostToDevice, st));
   }
 
-  void run(int mode, const hvm64_tuning* tp, double* device_ms) {
+  // Nets of the last run: [run_first, run_first + run_count).
+  unsigned run_first = 0, run_count = 0;
+
+  // Reduce nets [first, first + count) (count clamped to the batch); the
+  // other nets' results of earlier runs become unavailable.
+  void run(int mode, const hvm64_tuning* tp, double* device_ms, unsigned first = 0, unsigned count = ~0u) {
     hvm64_tuning t{};
     if (tp) t = *tp;
+    if (first > progs.size()) throw Error(HVM64_ERR_BAD_INPUT, "net range starts past the batch");
+    count = unsigned(std::min<uint64_t>(count, progs.size() - first));
+    run_first = first;
+    run_count = count;
     unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : DEFAULT_QLOG2;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
     h2d = d2h = 0;
@@ -1018,9 +1038,9 @@ struct Runner {
       }
     };
     if (mode == HVM64_BATCH_PLAIN) {
-      for (unsigned i = 0; i < progs.size(); i++) one(i, 1);
+      for (unsigned i = first; i < first + count; i++) one(i, 1);
     } else if (t.flags & HVM64_TUNE_GRAPH) {
-      total_ms = run_graph(t, qlog2, timeout_ms);
+      total_ms = run_graph(t, qlog2, timeout_ms, first, count);
       CU(cudaMemcpy(&host_ctrl, ctrl.p, sizeof host_ctrl, cudaMemcpyDeviceToHost));
       d2h += sizeof(dev::Ctrl);
       stat_donated += host_ctrl.stat_donated;
@@ -1032,11 +1052,11 @@ struct Runner {
       stat_idle += host_ctrl.stat_idle_cycles;
       bump = std::min<uint64_t>(host_ctrl.bump, heap_bytes / 16);
       if (host_ctrl.error) {
-        for (auto& n : host_nets) n.status = host_ctrl.error;
+        for (unsigned k = first; k < first + count; k++) host_nets[k].status = host_ctrl.error;
         note_error(host_ctrl);
       }
     } else {
-      one(0, unsigned(progs.size()));
+      one(first, count);
     }
     CU(cudaEventDestroy(e0));
     CU(cudaEventDestroy(e1));
@@ -1063,9 +1083,12 @@ struct Runner {
     if (!error_detail.empty()) return;
     if (h.error == HVM64_ERR_TIMEOUT)
       error_detail = h.error_info == 0
-                         ? " (a bounded wait gave up: a locked heap word, or a full redex queue; "
-                           "a larger tuning queue_slots_log2 helps the latter)"
+                         ? " (a bounded wait on a locked heap word gave up)"
                          : " (the run deadline, tuning timeout_ms, passed)";
+    else if (h.error == HVM64_ERR_QUEUE)
+      error_detail = " (net " + std::to_string(h.error_net) +
+                     (h.error_info == 2 ? ": the boot redexes" : ": a warp's overflow stack was full and") +
+                     " found the global redex queue full; a larger tuning queue_slots_log2 gives it more room)";
     else
       error_detail = " (net " + std::to_string(h.error_net) + ")";
   }
@@ -1094,20 +1117,20 @@ struct Runner {
     if (gs) cudaStreamDestroy(gs);
   }
 
-  float run_graph(const hvm64_tuning& t, unsigned qlog2, uint64_t timeout_ms) {
+  float run_graph(const hvm64_tuning& t, unsigned qlog2, uint64_t timeout_ms, unsigned first, unsigned count) {
     size_t qn = size_t(1) << qlog2;
-    unsigned count = unsigned(progs.size());
+    const unsigned n = unsigned(progs.size());
     std::vector<uint64_t> key = {t.blocks_per_sm, t.chunk_nodes, t.donate_min, qlog2, t.lane_budget, timeout_ms,
-                                 count, uint64_t(heap.p), uint64_t(q.p), uint64_t(d_defs.p), uint64_t(spill.p),
+                                 first, count, uint64_t(heap.p), uint64_t(q.p), uint64_t(d_defs.p), uint64_t(spill.p),
                                  spill_cap, grid};
     for (auto p : progs) key.push_back(p);
     if (!gs) CU(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
     if (!gexec || key != gkey) {
       drop_graph();
       CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_ctrl), sizeof(dev::Ctrl), cudaHostAllocDefault));
-      CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_nets), sizeof(dev::NetState) * std::max<size_t>(count, 1),
+      CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_nets), sizeof(dev::NetState) * std::max<size_t>(n, 1),
                        cudaHostAllocDefault));
-      memcpy(pin_nets, host_nets.data(), sizeof(dev::NetState) * count);
+      memcpy(pin_nets, host_nets.data(), sizeof(dev::NetState) * n);
       dev::Ctrl c{};
       c.bump = 1;
       c.heap_nodes = heap_bytes / 16;
@@ -1127,13 +1150,13 @@ struct Runner {
       auto step = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
       };
-      step(cudaMemcpyAsync(nets.p, pin_nets, sizeof(dev::NetState) * count, cudaMemcpyHostToDevice, gs));
+      step(cudaMemcpyAsync(nets.p, pin_nets, sizeof(dev::NetState) * n, cudaMemcpyHostToDevice, gs));
       step(cudaMemcpyAsync(ctrl.p, pin_ctrl, sizeof(dev::Ctrl), cudaMemcpyHostToDevice, gs));
       dev::queue_init_kernel<<<unsigned((qn + 255) / 256), 256, 0, gs>>>(q.p, qn);
       step(cudaGetLastError());
       dev::set_deadline_kernel<<<1, 1, 0, gs>>>(ctrl.p, c.timeout_ns);
       step(cudaGetLastError());
-      dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, gs>>>(p, 0, count);
+      dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, gs>>>(p, first, count);
       step(cudaGetLastError());
       dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, gs>>>(p);
       step(cudaGetLastError());
@@ -1158,7 +1181,7 @@ struct Runner {
     CU(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    h2d += sizeof(dev::NetState) * count + sizeof(dev::Ctrl);
+    h2d += sizeof(dev::NetState) * n + sizeof(dev::Ctrl);
     return ms;
   }
 
@@ -1193,15 +1216,19 @@ struct Runner {
   DevBuf<unsigned> d_gcount;
   DevBuf<dev::ull> d_goff, d_gpairs;
 
+  // Gathers the normal forms of the last run's nets (device-side walk).
   void gather_all() {
-    unsigned n = unsigned(progs.size());
+    const unsigned n = unsigned(progs.size()), first = run_first, cnt = run_count;
     const dev::Params p = params();
     d_gcount.alloc(n);
-    unsigned blocks = (n + 127) / 128;
-    dev::gather_kernel<<<blocks, 128>>>(p, n, d_gcount.p, nullptr, nullptr);
+    unsigned blocks = (cnt + 127) / 128;
+    gcount.assign(n, ~0u);
+    if (cnt) CU(cudaMemcpy(d_gcount.p, gcount.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    if (cnt) dev::gather_kernel<<<blocks, 128>>>(p, first, cnt, d_gcount.p, nullptr, nullptr);
     CU(cudaGetLastError());
-    gcount.resize(n);
     CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    for (unsigned i = 0; i < n; i++)
+      if (i < first || i >= first + cnt) gcount[i] = 0;  // not in this run: read back as an error
     goff.resize(n);
     uint64_t tot = 0;
     for (unsigned i = 0; i < n; i++) {
@@ -1211,29 +1238,32 @@ struct Runner {
     d_goff.alloc(n);
     CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
     d_gpairs.alloc(2 * tot);
-    dev::gather_kernel<<<blocks, 128>>>(p, n, d_gcount.p, d_goff.p, d_gpairs.p);
+    if (cnt) dev::gather_kernel<<<blocks, 128>>>(p, first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
     CU(cudaGetLastError());
     gpairs.resize(2 * tot);
     if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
     d2h += size_t(n) * 4 + 16 * tot;
     h2d += size_t(n) * 8;
     // Every gathered net's text at once, on the host's cores.
-    std::vector<uint64_t> roots(n);
-    for (unsigned i = 0; i < n; i++) roots[i] = host_nets[i].root;
+    std::vector<uint64_t> roots(cnt);
+    for (unsigned i = 0; i < cnt; i++) roots[i] = host_nets[first + i].root;
     unsigned hw = std::thread::hardware_concurrency();
-    gtext = readback_pairs_many(book, gpairs.data(), goff.data(), gcount.data(), roots.data(), n, heap_bytes / 8,
-                                std::max(1u, std::min(hw ? hw : 1u, 16u)));
+    gtext = readback_pairs_many(book, gpairs.data(), goff.data() + first, gcount.data() + first, roots.data(), cnt,
+                                heap_bytes / 8, std::max(1u, std::min(hw ? hw : 1u, 16u)));
     pairs_valid = true;
   }
   std::vector<ReadbackOut> gtext;
 
   std::string readback(unsigned i) {
     if (!reduced) throw Error(HVM64_ERR_BAD_INPUT, "net not reduced yet");
+    if (i < run_first || i >= run_first + run_count)
+      throw Error(HVM64_ERR_BAD_INPUT, "net " + std::to_string(i) + " was not in the last run's range");
     if (host_nets[i].status) throw Error(host_nets[i].status, status_name(host_nets[i].status));
     if (!pairs_valid) gather_all();
     if (gcount[i] != ~0u) {
-      if (!gtext[i].ok) throw Error(HVM64_ERR_BAD_INPUT, gtext[i].error);
-      return gtext[i].text;
+      const ReadbackOut& r = gtext[i - run_first];
+      if (!r.ok) throw Error(HVM64_ERR_BAD_INPUT, r.error);
+      return r.text;
     }
     if (!image_valid) {
       // Copy the used part of the heap (everything below the bump pointer).
@@ -1615,22 +1645,29 @@ int hvm64_batch_create(const hvm64_book* book, uint32_t n, const char* const* en
     *out = b.release();
   });
 }
-int hvm64_batch_normal(hvm64_batch* b, int mode, const hvm64_tuning* t, hvm64_rewrites* per_net, int* status,
-                       double* device_ms) {
+int hvm64_batch_normal_range(hvm64_batch* b, int mode, const hvm64_tuning* t, uint32_t first, uint32_t count,
+                             hvm64_rewrites* per_net, int* status, double* device_ms) {
   if (!b) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
   if (mode != HVM64_BATCH_PERSISTENT && mode != HVM64_BATCH_PLAIN)
     return hvm::set_error(HVM64_ERR_BAD_INPUT, "unknown batch mode");
-  int rc = guarded([&] { b->r.run(mode, t, device_ms); });
+  if (first > b->r.progs.size() || count > b->r.progs.size() - first)
+    return hvm::set_error(HVM64_ERR_BAD_INPUT, "net range outside the batch");
+  int rc = guarded([&] { b->r.run(mode, t, device_ms, first, count); });
   if (rc) return rc;
   int worst = 0;
-  for (size_t i = 0; i < b->r.host_nets.size(); i++) {
-    const auto& s = b->r.host_nets[i];
-    if (per_net) per_net[i] = hvm64_rewrites{s.rw[0], s.rw[1], s.rw[2], s.rw[3], s.rw[4]};
-    if (status) status[i] = s.status;
+  for (uint32_t k = 0; k < count; k++) {
+    const auto& s = b->r.host_nets[first + k];
+    if (per_net) per_net[k] = hvm64_rewrites{s.rw[0], s.rw[1], s.rw[2], s.rw[3], s.rw[4]};
+    if (status) status[k] = s.status;
     if (s.status && !worst) worst = s.status;
   }
   if (worst) return hvm::set_error(worst, b->r.error_message(worst));
   return HVM64_OK;
+}
+int hvm64_batch_normal(hvm64_batch* b, int mode, const hvm64_tuning* t, hvm64_rewrites* per_net, int* status,
+                       double* device_ms) {
+  if (!b) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return hvm64_batch_normal_range(b, mode, t, 0, uint32_t(b->r.progs.size()), per_net, status, device_ms);
 }
 int hvm64_batch_readback(hvm64_batch* b, uint32_t i, char* buf, size_t cap, size_t* len) {
   if (!b || i >= b->r.progs.size()) return hvm::set_error(HVM64_ERR_BAD_INPUT, "bad batch index");
@@ -1675,7 +1712,7 @@ int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
 namespace hvm {
 namespace noalloc {
 constexpr uint64_t SCRATCH_BYTES = uint64_t(64) << 20;  // 64 MiB in all
-constexpr unsigned QLOG2 = 12;                           // 4096 queue slots of 32 redexes
+constexpr unsigned QLOG2 = 13;                           // 8192 queue slots of 32 redexes
 // The reducer grid is capped at MAX_WARPS warps (4 blocks of 2 warps on
 // each of 148 SMs), each with an overflow stack of SPILL redexes, and lanes
 // take allocator chunks of CHUNK_NODES nodes: every lane holding a part-used
@@ -1723,8 +1760,8 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   hvm64_tuning t{};
   if (tp) t = *tp;
   if (t.queue_slots_log2 && t.queue_slots_log2 != QLOG2)
-    throw Error(HVM64_ERR_BAD_INPUT, "the no-allocation entry point has a fixed queue of 2^12 slots "
-                                     "(queue_slots_log2 must be 0 or 12)");
+    throw Error(HVM64_ERR_BAD_INPUT, "the no-allocation entry point has a fixed queue of 2^13 slots "
+                                     "(queue_slots_log2 must be 0 or 13)");
   auto it = book.ids.find(name);
   if (it == book.ids.end()) throw Error(HVM64_ERR_BAD_INPUT, std::string("no definition named @") + name);
   uint64_t defs_b = book.defs.size() * sizeof(DevDef), ins_b = book.instrs.size() * sizeof(DevInstr);

@@ -27,6 +27,7 @@ EXPORTS = (
     "hvm64_book_free", "hvm64_net_create", "hvm64_net_boot", "hvm64_net_encode", "hvm64_net_normal",
     "hvm64_net_readback", "hvm64_net_free", "hvm64_batch_create", "hvm64_batch_normal", "hvm64_batch_readback",
     "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats", "hvm64_net_normal_noalloc",
+    "hvm64_batch_normal_range",
     "hvm64_server_create", "hvm64_server_submit", "hvm64_server_poll", "hvm64_server_result", "hvm64_server_free",
 )
 
@@ -105,6 +106,8 @@ def lib(build_if_missing=True):
     L.hvm64_batch_create.argtypes = [P, c.c_uint32, c.POINTER(c.c_char_p), c.c_uint64, c.POINTER(P)]
     L.hvm64_batch_normal.argtypes = [P, c.c_int, c.POINTER(Tuning), c.POINTER(Rewrites), c.POINTER(c.c_int),
                                      c.POINTER(c.c_double)]
+    L.hvm64_batch_normal_range.argtypes = [P, c.c_int, c.POINTER(Tuning), c.c_uint32, c.c_uint32,
+                                           c.c_void_p, c.c_void_p, c.POINTER(c.c_double)]
     L.hvm64_batch_readback.argtypes = [P, c.c_uint32, c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_batch_free.argtypes = [P]
     L.hvm64_batch_stats.argtypes = [P, c.POINTER(Stats)]
@@ -211,10 +214,18 @@ class Batch:
         self.status = (ctypes.c_int * self.n)()
         self.device_ms = 0.0
 
-    def normal(self, mode=PERSISTENT, tuning=None, check=True):
+    def normal(self, mode=PERSISTENT, tuning=None, check=True, first=0, count=None):
+        """Reduce every net, or only nets [first, first + count) (one launch;
+        only those can be read back afterwards).  self.rwts[i] and
+        self.status[i] hold net i's results."""
         ms = ctypes.c_double()
         t = ctypes.byref(tuning) if tuning is not None else None
-        rc = lib().hvm64_batch_normal(self._h, mode, t, self.rwts, self.status, ctypes.byref(ms))
+        if count is None:
+            count = self.n - first
+        rsz, isz = ctypes.sizeof(Rewrites), ctypes.sizeof(ctypes.c_int)
+        per_net = ctypes.addressof(self.rwts) + first * rsz
+        status = ctypes.addressof(self.status) + first * isz
+        rc = lib().hvm64_batch_normal_range(self._h, mode, t, first, count, per_net, status, ctypes.byref(ms))
         self.device_ms = ms.value
         if check:
             _check(rc)

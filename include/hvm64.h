@@ -107,6 +107,12 @@ int hvm64_batch_create(const hvm64_book* book, uint32_t n, const char* const* en
  * counters, status (n entries, nullable) each net's status code. */
 int hvm64_batch_normal(hvm64_batch* batch, int mode, const hvm64_tuning* tuning, hvm64_rewrites* per_net,
                        int* status, double* device_ms);
+/* The same for nets [first, first + count) only, in one launch (persistent)
+ * or one per net (plain): per_net and status have `count` entries.  Only
+ * these nets can be read back afterwards.  No reference counterpart (a caller
+ * of the reference reduces one net per call). */
+int hvm64_batch_normal_range(hvm64_batch* batch, int mode, const hvm64_tuning* tuning, uint32_t first,
+                             uint32_t count, hvm64_rewrites* per_net, int* status, double* device_ms);
 int hvm64_batch_readback(hvm64_batch* batch, uint32_t i, char* buf, size_t cap, size_t* len);
 void hvm64_batch_free(hvm64_batch* batch);
 
