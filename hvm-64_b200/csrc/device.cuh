@@ -95,6 +95,8 @@ struct Ctrl {
   int stop;           // serving: the host asks the reducer to end once idle
   int pad7;
   ull pad8[14];
+  ull free_top;       // shared stack of free-node batches: batch head address | push count << 44
+  ull pad9[15];
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -339,6 +341,7 @@ struct WarpSmem {
   ull rw[NCOUNT];             // counters of the warp's current net
   unsigned cnt[NCOUNT * 32];  // per lane: counts of this step, [counter][lane] (folded into rw)
   ull ovf[32];                // per lane: overflow free list (left word links; right word LOCK)
+  unsigned ovf_n[32];         // per lane: nodes added to `ovf` since it was last published
   ull fw[4 * 32];             // per lane: words freed alone by the current interaction
   ull bnext[32], bend[32];    // per lane: pre-LOCKed bump chunk [bnext, bend), node indices
   unsigned allocs[32];        // per lane: nodes allocated (for the DREF statistics)
@@ -361,6 +364,7 @@ struct WarpSmem {
 HVM_INL void lane_init(WarpSmem* W, unsigned ln) {
   for (int k = 0; k < NCOUNT; k++) W->cnt[k * 32 + ln] = 0;
   W->ovf[ln] = 0;
+  W->ovf_n[ln] = 0;
   for (int k = 0; k < 4; k++) W->fw[k * 32 + ln] = 0;
   W->bnext[ln] = W->bend[ln] = 0;
   W->allocs[ln] = 0;
@@ -414,16 +418,64 @@ HVM_COLD uint32_t binary_op(unsigned net, uint32_t a, uint32_t op, uint32_t b) {
 // driver ships the redex to shared work (the CUDA driver: a one-redex queue
 // slot, or HVM64_ERR_QUEUE when the queue is full -- it never waits).
 HVM_COLD void push_overflow(unsigned net, ull a, ull b);
-// Pop the rare overflow free list / take a new pre-LOCKed bump chunk.
+// Free nodes move between warps through one shared stack of batches: a
+// lane's list of reclaimed nodes (linked through their left words, right
+// words LOCK) is published whole once it holds OVF_FLUSH nodes, the batch's
+// head node linking the next batch through its right word; a lane whose own
+// lists are empty takes a batch before it takes fresh nodes from the bump
+// pointer.  The top word carries a push/pop count above the address bits, so
+// a pop whose batch was taken and republished meanwhile fails its CAS (ABA).
+#ifndef HVM_OVF_FLUSH
+#define HVM_OVF_FLUSH 128
+#endif
+constexpr unsigned OVF_FLUSH = HVM_OVF_FLUSH;
+constexpr ull FT_ADDR = (1ull << 44) - 1;
+constexpr ull FT_TAG = 1ull << 44;
+HVM_COLD void free_publish(unsigned net, ull* ovf, unsigned* ovf_n) {
+  ull head = *ovf;
+  if (!head) return;
+  ull* top = &g_P.ctrl->free_top;
+  unsigned it = 0;
+  for (;;) {
+    ull t = ld_gpu(top);
+    st_gpu(heap_at(net, head | 8), t & FT_ADDR);
+    mem_fence();  // the batch's links are visible before its head is
+    if (atom_cas(top, t, (head & FT_ADDR) | ((t & ~FT_ADDR) + FT_TAG)) == t) break;
+    if (!run_spin(net, it)) return;  // lost CASes are other lanes' progress; still bounded
+  }
+  *ovf = 0;
+  *ovf_n = 0;
+}
+// Take one batch from the shared stack as the lane's list; false when empty.
+HVM_COLD bool free_take(unsigned net, ull* ovf) {
+  ull* top = &g_P.ctrl->free_top;
+  for (int tries = 0; tries < 64; tries++) {
+    ull t = ld_gpu(top);
+    ull a = t & FT_ADDR;
+    if (a == 0) return false;
+    // Stale when the batch was taken meanwhile; then the CAS below fails.
+    ull next = ld_gpu(heap_at(net, a | 8));
+    if (atom_cas(top, t, (next & FT_ADDR) | ((t & ~FT_ADDR) + FT_TAG)) == t) {
+      mem_fence();
+      st_gpu(heap_at(net, a | 8), P_LOCK);
+      *ovf = a;
+      return true;
+    }
+  }
+  return false;
+}
+// Pop the lane's free list (or a shared batch) / take a new pre-LOCKed bump
+// chunk.
 struct Refill {
   ull node, bnext, bend;
 };
-HVM_COLD Refill alloc_refill(unsigned net, ull* ovf) {
-  if (*ovf != 0) {
+HVM_COLD Refill alloc_refill(unsigned net, ull* ovf, unsigned* ovf_n) {
+  if (*ovf != 0 || free_take(net, ovf)) {
     ull a = *ovf;
     *ovf = ld_gpu(heap_at(net, a));
     st_gpu(heap_at(net, a), P_LOCK);
     mem_fence();
+    if (*ovf_n) --*ovf_n;
     return {a, 0, 0};
   }
   ull n = g_P.ctrl->chunk_nodes;
@@ -435,6 +487,12 @@ HVM_COLD Refill alloc_refill(unsigned net, ull* ovf) {
   lock_fill(g_P.heap, s, n);
   mem_fence();  // LOCK is visible before any of these nodes escapes
   return {s << 4, s + 1, s + n};
+}
+// A reclaimed node (both words LOCK) onto a lane's free list.
+HVM_INL void free_list_push(unsigned net, ull* ovf, unsigned* ovf_n, ull node) {
+  st_gpu(heap_at(net, node), *ovf);
+  *ovf = node;
+  if (++*ovf_n >= OVF_FLUSH) free_publish(net, ovf, ovf_n);
 }
 
 // ---- the runtime proper ------------------------------------------------------
@@ -513,12 +571,11 @@ HVM_COLD void recycle(const Ctx& c, ull node) {
   if (k < c.W->pool_cap) {
     c.W->freed[k] = node;
   } else {
-    hstore(c, node, LS(ovf));  // right word already LOCK
-    LS(ovf) = node;
+    free_list_push(c.net, &LS(ovf), &LS(ovf_n), node);  // right word already LOCK
   }
 }
 HVM_COLD ull alloc_slow(const Ctx& c) {
-  Refill r = alloc_refill(c.net, &LS(ovf));
+  Refill r = alloc_refill(c.net, &LS(ovf), &LS(ovf_n));
   if (r.bend) {
     LS(bnext) = r.bnext;
     LS(bend) = r.bend;

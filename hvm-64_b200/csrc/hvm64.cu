@@ -219,6 +219,37 @@ __global__ void gather_kernel(const __grid_constant__ Params P, unsigned first, 
   }
 }
 
+// After a served net's normal form is gathered, nothing refers to its nodes
+// any more: every node the normal form reaches (through principal ports, as
+// the gather walks it) and the root node go back on lane 0's free list, so a
+// long-running server reuses them for later requests.  The walk uses the
+// warp's ring as its stack; a normal form deeper than that keeps the rest.
+__device__ __noinline__ void serve_release(WarpSmem& W, unsigned slot, ull root) {
+  ull* stk = W.stk;
+  const unsigned cap = 2 * SCAP;
+  unsigned sp = 0;
+  ull w0 = ld_gpu(heap_at(slot, root));
+  auto visit = [&](ull v) {
+    unsigned t = unsigned(v & 7);
+    if ((t == T_OP || t == T_CTR || t == T_SWITCH) && sp < cap) stk[sp++] = paddr(v);
+  };
+  visit(w0);
+  for (unsigned guard = 0; sp && guard < (1u << 24); guard++) {
+    ull a = stk[--sp];
+    ull l = ld_gpu(heap_at(slot, a)), r = ld_gpu(heap_at(slot, a | 8));
+    visit(l);
+    visit(r);
+    st_gpu(heap_at(slot, a | 8), P_LOCK);
+    free_list_push(slot, &W.ovf[0], &W.ovf_n[0], a);
+  }
+  // the root node: its left word held the root wire, its right half was
+  // freed when the root was allocated (runtime/src/net.rs:65-69)
+  ull rn = root & ~8ull;
+  st_gpu(heap_at(slot, rn | 8), P_LOCK);
+  free_list_push(slot, &W.ovf[0], &W.ovf_n[0], rn);
+  mem_fence();
+}
+
 // The net in `slot` reached normal form: gather it and post its completion
 // record (the ticket last, after a system-scope fence).  Lane 0 only.
 __device__ __noinline__ void serve_complete(WarpSmem& W, unsigned slot) {
@@ -238,6 +269,7 @@ __device__ __noinline__ void serve_complete(WarpSmem& W, unsigned slot) {
   __threadfence_system();
   d->ticket = ld_gpu(&ns.ticket);
   __threadfence_system();
+  if (status == 0) serve_release(W, slot, root);
 }
 
 // Take the next request, if the host has written one, and boot it in this
@@ -280,6 +312,7 @@ __device__ __noinline__ unsigned serve_admit(WarpSmem& W, Ctx& c) {
   W.ring_cap = unsigned(SCAP - HEADROOM);
   W.ring_cnt = 0;
   ull root = alloc(c);
+  half_free(c, root ^ 8);  // only the left word is the root wire; the node is reclaimed once it is freed
   if (prog < g_P.ndefs && !(g_P.defs[prog].flags & 1)) W.rw[RW_DREF]++;
   run_def(c, prog, pvar(root));
   settle(c);
@@ -641,9 +674,7 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_
       for (int i = int(lane); i < mv; i += 32) W.pool[pn + i] = W.freed[i];
       for (int i = mv + int(lane); i < fn; i += 32) {
         // pool full: the rest goes to this lane's overflow list
-        ull node = W.freed[i];
-        st_gpu(heap_at(unsigned(cur), node), W.ovf[lane]);
-        W.ovf[lane] = node;
+        free_list_push(unsigned(cur), &W.ovf[lane], &W.ovf_n[lane], W.freed[i]);
       }
       __syncwarp();
       if (lane == 0) {
@@ -1325,7 +1356,9 @@ struct Server {
   bool running = false;
   uint64_t tail = 0, next_ticket = 1;
   std::vector<uint64_t> slot_ticket;  // 0: free
+  std::vector<uint64_t> slot_nodes;   // the node budget each slot's request holds
   std::vector<unsigned> free_slots;
+  uint64_t budget_nodes = 0, reserved_nodes = 0;
 
   ~Server() { shutdown(); }
 
@@ -1358,8 +1391,8 @@ struct Server {
     CU(cudaHostAlloc(reinterpret_cast<void**>(&out), sizeof(dev::ull) * 2 * size_t(out_cap) * nslots,
                      cudaHostAllocMapped));
     CU(cudaHostAlloc(reinterpret_cast<void**>(&req_stage), sizeof(dev::ServeReq) * req_cap, cudaHostAllocDefault));
-    CU(cudaHostAlloc(reinterpret_cast<void**>(&tail_stage), sizeof(uint64_t) * req_cap, cudaHostAllocDefault));
-    CU(cudaHostAlloc(reinterpret_cast<void**>(&stop_stage), sizeof(int), cudaHostAllocDefault));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&tail_stage), sizeof(uint64_t) * (req_cap + 1), cudaHostAllocDefault));
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&stop_stage), 2 * sizeof(int), cudaHostAllocDefault));
     memset(done, 0, sizeof(dev::ServeDone) * nslots);
     *stop_stage = 0;
     dev::ServeDone* d_done = nullptr;
@@ -1380,7 +1413,9 @@ struct Server {
     c.bump = 1;
     c.heap_nodes = heap_bytes / 16;
     c.heap_bytes = heap_bytes;
-    c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
+    // small allocator chunks: a server's heap is shared by requests for its
+    // whole life, so nodes stranded in part-used chunks count against it
+    c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 32;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
     c.lane_budget = t.lane_budget ? t.lane_budget : 1;
@@ -1410,6 +1445,16 @@ struct Server {
     p.out_cap = out_cap;
     const unsigned grid = unsigned(sms * reducer_blocks_per_sm(t));
     const uint64_t warps = uint64_t(grid) * dev::WARPS;
+    // Node budget for admission: the heap minus what the allocator can hold
+    // back while nothing is live (each lane's part-used chunk and unpublished
+    // free list, each warp's reuse pool).
+    const uint64_t reserve = warps * 32 * (c.chunk_nodes + dev::OVF_FLUSH) + warps * dev::POOL;
+    if (heap_bytes / 16 <= 2 * reserve)
+      throw Error(HVM64_ERR_BAD_INPUT, "heap_bytes too small for a server: its allocator may hold back " +
+                                           std::to_string(reserve) + " nodes; give it at least " +
+                                           std::to_string(2 * reserve * 16) + " bytes");
+    budget_nodes = heap_bytes / 16 - reserve;
+    reserved_nodes = 0;
     p.spill_cap = spill_cap_for(heap_bytes, warps);
     spill.alloc(2 * size_t(p.spill_cap) * warps);
     p.spill = spill.p;
@@ -1418,6 +1463,7 @@ struct Server {
     CU(cudaGetLastError());
     running = true;
     slot_ticket.assign(nslots, 0);
+    slot_nodes.assign(nslots, 0);
     free_slots.clear();
     for (unsigned i = nslots; i-- > 0;) free_slots.push_back(i);
   }
@@ -1433,15 +1479,26 @@ struct Server {
     return e;
   }
 
-  uint64_t submit(const std::string& name) {
+  // Admits a request that may hold up to `nodes` live heap nodes (0: an
+  // even share of the budget, budget / slots) when a slot and that much of
+  // the node budget are free.
+  uint64_t submit(const std::string& name, uint64_t nodes) {
     if (!running) throw Error(HVM64_ERR_BAD_INPUT, "server is not running");
     auto it = book.ids.find(name);
     if (it == book.ids.end()) throw Error(HVM64_ERR_BAD_INPUT, "no definition named @" + name);
     if (free_slots.empty()) throw Error(HVM64_ERR_QUEUE, "no free slot: poll and collect results first");
+    if (nodes == 0) nodes = std::max<uint64_t>(1, budget_nodes / nslots);
+    if (nodes > budget_nodes)
+      throw Error(HVM64_ERR_BAD_INPUT, "request needs " + std::to_string(nodes) + " nodes; the server's budget is " +
+                                           std::to_string(budget_nodes));
+    if (reserved_nodes + nodes > budget_nodes)
+      throw Error(HVM64_ERR_QUEUE, "not enough free node budget: poll and collect results first");
     unsigned slot = free_slots.back();
     free_slots.pop_back();
     uint64_t ticket = next_ticket++;
     slot_ticket[slot] = ticket;
+    slot_nodes[slot] = nodes;
+    reserved_nodes += nodes;
     unsigned k = unsigned(tail % req_cap);
     req_stage[k] = dev::ServeReq{ticket, slot, it->second};
     CU(cudaMemcpyAsync(req.p + k, req_stage + k, sizeof(dev::ServeReq), cudaMemcpyHostToDevice, cs));
@@ -1449,6 +1506,15 @@ struct Server {
     CU(cudaMemcpyAsync(&ctrl.p->req_tail, tail_stage + k, 8, cudaMemcpyHostToDevice, cs));
     CU(cudaStreamSynchronize(cs));
     return ticket;
+  }
+
+  // Nodes ever taken from the bump pointer (the heap's high-water mark),
+  // read while the reducer runs.
+  uint64_t heap_high() {
+    if (!running) return 0;
+    CU(cudaMemcpyAsync(tail_stage + req_cap, &ctrl.p->bump, 8, cudaMemcpyDeviceToHost, cs));
+    CU(cudaStreamSynchronize(cs));
+    return tail_stage[req_cap];
   }
 
   size_t poll(uint64_t* tickets, size_t cap) {
@@ -1477,14 +1543,21 @@ struct Server {
       with_big_stack([&] { text = readback_pairs(book, pairs.data(), d->pairs, heap_bytes / 8, root); });
     }
     slot_ticket[s] = 0;
+    reserved_nodes -= slot_nodes[s];
+    slot_nodes[s] = 0;
     free_slots.push_back(s);
     return status;
   }
 
+  // Stops the reducer at once: `stop` ends idle warps, and the run's error
+  // word (which every warp polls between steps) ends warps still reducing
+  // requests, whose results are abandoned.
   void shutdown() {
     if (running) {
-      *stop_stage = 1;
+      stop_stage[0] = 1;
+      stop_stage[1] = HVM64_ERR_TIMEOUT;
       cudaMemcpyAsync(&ctrl.p->stop, stop_stage, sizeof(int), cudaMemcpyHostToDevice, cs);
+      cudaMemcpyAsync(&ctrl.p->error, stop_stage + 1, sizeof(int), cudaMemcpyHostToDevice, cs);
       cudaStreamSynchronize(cs);
       cudaStreamSynchronize(ks);
       running = false;
@@ -1881,8 +1954,19 @@ int hvm64_server_create(const hvm64_book* book, uint64_t heap_bytes, uint32_t sl
   });
 }
 int hvm64_server_submit(hvm64_server* sv, const char* def_name, uint64_t* ticket) {
+  return hvm64_server_submit_nodes(sv, def_name, 0, ticket);
+}
+int hvm64_server_submit_nodes(hvm64_server* sv, const char* def_name, uint64_t nodes, uint64_t* ticket) {
   if (!sv || !def_name || !ticket) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
-  return guarded([&] { *ticket = sv->s.submit(def_name); });
+  return guarded([&] { *ticket = sv->s.submit(def_name, nodes); });
+}
+int hvm64_server_budget(hvm64_server* sv, uint64_t* budget, uint64_t* reserved, uint64_t* heap_high) {
+  if (!sv) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] {
+    if (budget) *budget = sv->s.budget_nodes;
+    if (reserved) *reserved = sv->s.reserved_nodes;
+    if (heap_high) *heap_high = sv->s.heap_high();
+  });
 }
 int hvm64_server_poll(hvm64_server* sv, uint64_t* tickets, size_t cap, size_t* n) {
   if (!sv || !n || (cap && !tickets)) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");

@@ -29,6 +29,7 @@ EXPORTS = (
     "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats", "hvm64_net_normal_noalloc",
     "hvm64_batch_normal_range",
     "hvm64_server_create", "hvm64_server_submit", "hvm64_server_poll", "hvm64_server_result", "hvm64_server_free",
+    "hvm64_server_submit_nodes", "hvm64_server_budget",
 )
 
 
@@ -116,6 +117,8 @@ def lib(build_if_missing=True):
                                            c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_server_create.argtypes = [P, c.c_uint64, c.c_uint32, c.c_uint32, c.POINTER(Tuning), c.POINTER(P)]
     L.hvm64_server_submit.argtypes = [P, c.c_char_p, c.POINTER(c.c_uint64)]
+    L.hvm64_server_submit_nodes.argtypes = [P, c.c_char_p, c.c_uint64, c.POINTER(c.c_uint64)]
+    L.hvm64_server_budget.argtypes = [P, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     L.hvm64_server_poll.argtypes = [P, c.POINTER(c.c_uint64), c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_server_result.argtypes = [P, c.c_uint64, c.POINTER(Rewrites), c.POINTER(c.c_int),
                                       c.POINTER(c.c_double), c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
@@ -247,9 +250,11 @@ class Batch:
 
 class Server:
     """A reducer that stays on the device and admits requests while it runs.
-    `submit(name)` boots Def `name` and returns a ticket; `poll()` lists
-    finished tickets; `result(ticket)` returns (text, Rewrites, device_us).
-    While it runs, no other entry point may be used on the same device."""
+    `submit(name, nodes=0)` boots Def `name` when a slot and `nodes` of the
+    node budget are free (ERR_QUEUE otherwise) and returns a ticket; `poll()`
+    lists finished tickets; `result(ticket)` returns (text, Rewrites,
+    device_us); `budget()` the node budget, its reserved part and the heap's
+    high-water mark.  `close()` stops the reducer at once."""
 
     def __init__(self, book, slots=256, out_pairs=1 << 16, heap_bytes=0, tuning=None):
         self.book = book
@@ -260,10 +265,15 @@ class Server:
         self._h = h
         self._buf = (ctypes.c_uint64 * slots)()
 
-    def submit(self, name):
+    def submit(self, name, nodes=0):
         t = ctypes.c_uint64()
-        _check(lib().hvm64_server_submit(self._h, name.encode(), ctypes.byref(t)))
+        _check(lib().hvm64_server_submit_nodes(self._h, name.encode(), nodes, ctypes.byref(t)))
         return t.value
+
+    def budget(self):
+        b, r, h = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().hvm64_server_budget(self._h, ctypes.byref(b), ctypes.byref(r), ctypes.byref(h)))
+        return {"budget": b.value, "reserved": r.value, "heap_high": h.value}
 
     def poll(self):
         n = ctypes.c_size_t()

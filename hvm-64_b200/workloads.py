@@ -257,24 +257,37 @@ def est_interactions(kind, depth):
 def serving_requests(n, seed=0, lo=1e3, hi=1e8):
     """The serving stream's requests: (kind, param, j) with a target size drawn
     log-uniform in [lo, hi] interactions; kind tree-sum / bitonic sort /
-    Church (47/47/6).  param is the depth (sum, sort) or (k, last) (Church:
-    k = 4 below 1e5 interactions, else the 524,508-interaction k = 5)."""
+    Church (47/47/6).  param is the depth (sum: up to 21, 1.1e8 interactions;
+    sort: up to 14, 7e7) or (k, last) (Church: k = 4 below 1e5 interactions,
+    else the 524,508-interaction k = 5)."""
     rng = random.Random(splitmix64(BASE_SEED ^ (0x5E4E + seed)))
     out = []
     for j in range(n):
         size = math.exp(rng.uniform(math.log(lo), math.log(hi)))
         r = rng.random()
         if r < 0.47:
-            d = max(3, min(20, int(round(math.log2(size / 54)))))
+            d = max(3, min(21, int(round(math.log2(size / 54)))))
             out.append(("sum", d, j))
         elif r < 0.94:
             d = 2
-            while d < 13 and est_interactions("sort", d) < size:
+            while d < 14 and est_interactions("sort", d) < size:
                 d += 1
             out.append(("sort", d, j))
         else:
             out.append(("church", (4, 2 + j % 4) if size < 1e5 else (5, 2), j))
     return out
+
+
+def est_request_interactions(kind, param):
+    if kind == "church":
+        return 6e4 if param[0] == 4 else 5.3e5
+    return est_interactions(kind, param)
+
+
+def est_request_nodes(kind, param):
+    """A generous bound on a request's live heap nodes, for admission by node
+    budget: an eighth of its interactions plus a floor."""
+    return int(est_request_interactions(kind, param) / 8) + 4096
 
 
 def serving_book(reqs):

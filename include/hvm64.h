@@ -11,7 +11,8 @@
  *    message of the last failure on the calling thread.
  *  - Handles are owned by the caller and released with the *_free calls.
  *    One handle is used by one host thread at a time (the reference's
- *    `&mut Net`).
+ *    `&mut Net`); different handles may be used from different threads at
+ *    once, on one device or several (each launch carries its own parameters).
  *  - A net's heap, redex queue and Book tables live in device memory behind
  *    the handle; buffers in these signatures are host memory.
  *  - No torch or CUDA types appear here; the library picks the current CUDA
@@ -143,11 +144,11 @@ int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
  * hvm64_server_poll writes up to `cap` finished tickets; hvm64_server_result
  * gives a finished request's Rewrites, status, device latency (admission to
  * completion, microseconds) and normal form (hvm64_net_readback's text
- * convention) and frees its slot.  hvm64_server_free stops the reducer once
- * every submitted request is done.
+ * convention) and frees its slot.  hvm64_server_free stops the reducer at
+ * once; requests still running are abandoned.
  *
- * While a server runs on a device, use no other entry point on that device
- * (they share the reducer's launch parameters).  An error in any request
+ * A server's reducer occupies every SM while it runs, so other entry points
+ * on that device wait for SMs (they stay correct).  An error in any request
  * (OOM, DIV0, BAD_PAIR, ...) stops the whole server; poll then returns it.
  * A server lives at most tuning->timeout_ms (default 10 minutes), then stops
  * with HVM64_ERR_TIMEOUT. */
@@ -155,6 +156,18 @@ typedef struct hvm64_server hvm64_server;
 int hvm64_server_create(const hvm64_book* book, uint64_t heap_bytes, uint32_t slots, uint32_t out_pairs,
                         const hvm64_tuning* tuning, hvm64_server** out);
 int hvm64_server_submit(hvm64_server* server, const char* def_name, uint64_t* ticket);
+/* Admission by node budget: the request may hold up to `nodes` live heap
+ * nodes (0: budget / slots, what hvm64_server_submit reserves).  The budget is
+ * the heap less what the allocator can hold back (per-lane chunks and free
+ * lists, per-warp pools); a request is admitted when a slot and `nodes` of the
+ * budget are free (else HVM64_ERR_QUEUE: collect results and retry), and its
+ * reservation returns with its result.  Nodes a finished request's normal
+ * form used are recycled for later requests, so a long-running server's heap
+ * stays bounded by what its requests hold at once. */
+int hvm64_server_submit_nodes(hvm64_server* server, const char* def_name, uint64_t nodes, uint64_t* ticket);
+/* The node budget, the part admitted requests hold, and the heap's high-water
+ * mark (nodes ever taken from fresh memory). */
+int hvm64_server_budget(hvm64_server* server, uint64_t* budget, uint64_t* reserved, uint64_t* heap_high);
 int hvm64_server_poll(hvm64_server* server, uint64_t* tickets, size_t cap, size_t* n);
 int hvm64_server_result(hvm64_server* server, uint64_t ticket, hvm64_rewrites* out, int* status,
                         double* device_us, char* buf, size_t cap, size_t* len);
@@ -169,21 +182,27 @@ void hvm64_server_free(hvm64_server* server);
  * audited device-memory budget, or a request loop that must not pay
  * cudaMalloc's latency and implicit device-wide synchronisation per request.
  * hvm64_net_create allocates a heap of its own; this call instead uses one
- * array compiled into the library
- * (64 MiB on every GPU that loads it, held until the process exits): a 4 MiB
- * region for the Book's device tables, a 4096-slot redex queue and a heap of
- * about 3.7 million nodes.  A Book whose tables exceed 4 MiB is refused with
- * HVM64_ERR_BAD_INPUT, a net that outgrows the heap stops with HVM64_ERR_OOM,
- * and tuning->queue_slots_log2 must be 0 or 12.  Host memory is used only to
+ * array compiled into the library (64 MiB on every GPU that loads it, held
+ * until the process exits): a 4 MiB region for the Book's device tables, a
+ * redex queue of 2^13 slots, overflow stacks for a reducer grid of at most
+ * 1184 warps (4 blocks of 2 warps per SM on 148 SMs), and a heap of
+ * 3,350,416 nodes.  Lanes take allocator chunks of 8 nodes, so part-used
+ * chunks tie up at most 303,104 of them; nodes a warp frees are reused by
+ * that warp.  Limits: a Book whose tables exceed 4 MiB is refused with
+ * HVM64_ERR_BAD_INPUT; a net that outgrows the heap stops with HVM64_ERR_OOM;
+ * a net whose waiting redexes outgrow the overflow stacks and the queue stops
+ * with HVM64_ERR_QUEUE; tuning->queue_slots_log2 must be 0 or 13 and
+ * tuning->blocks_per_sm above 4 counts as 4.  Host memory is used only to
  * render the normal-form text.
  *
  * The first call on a device looks up the array's device address (with that
  * device current); make that first call before any stream capture.  Every call
  * on a device shares the array and starts by resetting the parts a run reads
- * (control block, net record, queue, Book tables), so calls that overlap on
- * the GPU (from two host threads) race and must be serialised by the caller.
- * Outputs: `out` (nullable) receives the Rewrites; the normal form is written
- * as hvm64_net_readback writes it (buf/cap/len). */
+ * (control block, net record, queue, Book tables), so two of these calls that
+ * overlap on the GPU (from two host threads) race and must be serialised by
+ * the caller; other entry points use memory of their own and do not race with
+ * it.  Outputs: `out` (nullable) receives the Rewrites; the normal form is
+ * written as hvm64_net_readback writes it (buf/cap/len). */
 int hvm64_net_normal_noalloc(const hvm64_book* book, const char* def_name, const hvm64_tuning* tuning,
                              hvm64_rewrites* out, char* buf, size_t cap, size_t* len);
 

@@ -69,9 +69,12 @@ void give(Emu* E, WarpSmem& W, unsigned& bot, unsigned cnt, int cur) {
 // slots) so that pushes keep spilling into the overflow stack, whose own
 // small capacity sends the rest to the shared queue -- the paths a reducer
 // warp takes only under a burst of redexes.
-void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap) {
+void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsigned index) {
   g_emu = E;
   auto W = new_warp();
+  // Every other lane has no reuse pool: its reclaimed nodes all go through
+  // its free list and, in batches, the shared free stack.
+  if (index & 1) W->pool_cap = 0;
   std::vector<ull> spill(2 * size_t(spill_cap) + 2);
   W->sp = spill_cap ? spill.data() : nullptr;
   W->sp_cap = spill_cap;
@@ -139,8 +142,7 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap) {
     int pn = std::max(W->pool_n, 0), fn = std::min(W->freed_n, POOL), mv = std::min(fn, POOL - pn);
     for (int k = 0; k < mv; k++) W->pool[pn + k] = W->freed[k];
     for (int k = mv; k < fn; k++) {
-      hstore(c, W->freed[k], W->ovf[0]);
-      W->ovf[0] = W->freed[k];
+      free_list_push(c.net, &W->ovf[0], &W->ovf_n[0], W->freed[k]);
     }
     W->pool_n = pn + mv;
     W->freed_n = 0;
@@ -219,7 +221,7 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
       if (E.nets[0].pending > 0) E.C.nets_left = 1;
     }
     std::vector<std::thread> th;
-    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min, std::max(1u, ring), spill_cap);
+    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min, std::max(1u, ring), spill_cap, t);
     for (auto& t : th) t.join();
     if (E.C.error) {
       snprintf(err, errcap, "device error %d info 0x%llx", E.C.error, (unsigned long long)E.C.error_info);

@@ -1,6 +1,7 @@
 """The device runtime (hvm-64_b200/csrc/device.cuh) compiled for the host and
 run on many threads with random jitter in its memory operations: the link /
-redirect protocol, the allocator and the instruction VM must give the
+redirect protocol, the allocator (with free-node batches published to the
+shared stack after every 4 nodes) and the instruction VM must give the
 reference's normal forms and counts under contention.  CPU-only."""
 import ctypes
 import json
@@ -21,6 +22,7 @@ PROGRAMS = json.load(open(os.path.join(HERE, "golden", "programs.json")))
 def _lib():
     if not os.path.exists(SO) or any(os.path.getmtime(d) > os.path.getmtime(SO) for d in DEPS):
         subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", "-DHVM_EMU_STRESS",
+                        "-DHVM_OVF_FLUSH=4",
                         "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "hvm-64_b200", "csrc"),
                         *SRC, "-o", SO], check=True)
     L = ctypes.CDLL(SO)

@@ -101,7 +101,7 @@ def test_server_error_stops_it_cleanly():
     hvm64 = _hvm()
     src = "@bad = x & 10 ~ $([/] $(0 x))\n@ok = x & 3 ~ $([*] $(5 x))\n"
     book = hvm64.Book.from_str(src)
-    sv = hvm64.Server(book, slots=4, out_pairs=1 << 10, heap_bytes=1 << 28, tuning=hvm64.Tuning(timeout_ms=60000))
+    sv = hvm64.Server(book, slots=4, out_pairs=1 << 10, heap_bytes=1 << 30, tuning=hvm64.Tuning(timeout_ms=60000))
     try:
         sv.submit("bad")
         deadline = time.time() + 30
@@ -115,3 +115,80 @@ def test_server_error_stops_it_cleanly():
         sv.close()
     got, _ = hvm64.run_book(src.replace("@ok", "@main"), heap_bytes=1 << 24)
     assert got == "15"
+
+
+@pytest.mark.gpu
+def test_server_long_run_heap_stays_bounded():
+    """600 bitonic-sort requests (2^12 keys each; about 12,000 nodes of
+    normal form per request) through one server, 32 at a time, each admitted
+    against the node budget: every result is right, the reservation returns
+    to zero, and the heap's high-water mark after the first 60 requests grows
+    by far less than the 6.6 million nodes the later normal forms would hold
+    if finished requests' nodes were not recycled."""
+    hvm64 = _hvm()
+    reqs = [("sort", 12, j) for j in range(8)]
+    book = hvm64.Book.from_str(W.serving_book(reqs))
+    sv = hvm64.Server(book, slots=32, out_pairs=1 << 16, heap_bytes=4 << 30,
+                      tuning=hvm64.Tuning(timeout_ms=300000))
+    try:
+        owner, done, submitted, high_60 = {}, 0, 0, None
+        per_req = 200_000
+        deadline = time.time() + 240
+        while done < 600 and time.time() < deadline:
+            while submitted < 600:
+                try:
+                    t = sv.submit(f"main_{submitted % 8}", nodes=per_req)
+                except hvm64.HvmError as e:
+                    assert e.code == hvm64.ERR_QUEUE
+                    break
+                owner[t] = submitted % 8
+                submitted += 1
+            for t in sv.poll():
+                text, rw, us = sv.result(t)
+                j = owner.pop(t)
+                assert W.leaves(text) == sorted(W.sort_keys(12, j))
+                done += 1
+                if done == 60:
+                    high_60 = sv.budget()["heap_high"]
+            time.sleep(0.001)
+        assert done == 600
+        b = sv.budget()
+        assert b["reserved"] == 0
+        assert b["heap_high"] - high_60 < 3_000_000, (high_60, b)
+    finally:
+        sv.close()
+
+
+@pytest.mark.gpu
+def test_server_admits_by_node_budget():
+    """With slots to spare, requests are admitted only while their declared
+    node needs fit the free budget: the third of three requests that each
+    hold 40% of the budget is refused until a result is collected, and a
+    request larger than the whole budget is refused outright."""
+    hvm64 = _hvm()
+    reqs = [("sum", 10, j) for j in range(4)]
+    book = hvm64.Book.from_str(W.serving_book(reqs))
+    sv = hvm64.Server(book, slots=16, out_pairs=1 << 10, heap_bytes=1 << 30, tuning=hvm64.Tuning(timeout_ms=120000))
+    try:
+        budget = sv.budget()["budget"]
+        big = int(budget * 0.4)
+        owner = {sv.submit("main_0", nodes=big): 0, sv.submit("main_1", nodes=big): 1}
+        assert sv.budget()["reserved"] == 2 * big
+        with pytest.raises(hvm64.HvmError) as e:
+            sv.submit("main_2", nodes=big)
+        assert e.value.code == hvm64.ERR_QUEUE and "budget" in str(e.value)
+        with pytest.raises(hvm64.HvmError) as e:
+            sv.submit("main_3", nodes=budget + 1)
+        assert e.value.code == hvm64.ERR_BAD_INPUT
+        got = {}
+        _drain(sv, 1, got, time.time() + 30)
+        for t, (text, rw, us) in got.items():
+            assert text == str(W.expected_sum(10, owner.pop(t)))
+        owner[sv.submit("main_2", nodes=big)] = 2
+        got = {}
+        _drain(sv, 2, got, time.time() + 30)
+        for t, (text, rw, us) in got.items():
+            assert text == str(W.expected_sum(10, owner.pop(t)))
+        assert sv.budget()["reserved"] == 0
+    finally:
+        sv.close()

@@ -88,7 +88,7 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
         hvm64.normal_noalloc(big, "main")
     assert e.value.code == hvm64.ERR_BAD_INPUT and "too large" in str(e.value)
     # a net that outgrows the built-in heap (a generated tree of 2^22 leaves,
-    # kept whole: far more than its 3.49 million nodes) stops with OOM, and
+    # kept whole: far more than its 3.35 million nodes) stops with OOM, and
     # the next call works
     gen_only = W.tree_sum(22, 0).replace("@main = a\n& @sum ~ (b a)\n& @gen ~ (22 (0 b))",
                                          "@main = a\n& @gen ~ (22 (0 a))")
