@@ -84,10 +84,19 @@ void print_stats(const hvm64_rewrites& rw, double ms) {
   const char* names[] = {"RWTS   ", "- ANNI ", "- COMM ", "- ERAS ", "- DREF ", "- OPER "};
   unsigned long long vals[] = {total, rw.anni, rw.comm, rw.eras, rw.dref, rw.oper};
   for (int i = 0; i < 6; i++) fprintf(stderr, "%s: %15s\n", names[i], pretty(vals[i]).c_str());
-  double s = ms / 1000.0;
-  fprintf(stderr, "TIME   : %.3fs\n", s);
+  // TIME: a Duration's `{:.3?}`, i.e. in the largest unit whose whole part is
+  // nonzero (s, ms, µs, ns), three decimals.
+  double ns = ms * 1e6;
+  if (ns >= 1e9) fprintf(stderr, "TIME   : %.3fs\n", ns / 1e9);
+  else if (ns >= 1e6) fprintf(stderr, "TIME   : %.3fms\n", ns / 1e6);
+  else if (ns >= 1e3) fprintf(stderr, "TIME   : %.3f\xc2\xb5s\n", ns / 1e3);
+  else fprintf(stderr, "TIME   : %.3fns\n", ns);
+  // RPS: total / whole milliseconds / 1000 as an f64 (inf or NaN under 1 ms)
   double whole_ms = floor(ms);
-  fprintf(stderr, "RPS    : %.3f M\n", whole_ms > 0 ? double(total) / whole_ms / 1000.0 : 0.0);
+  double rps = whole_ms > 0 ? double(total) / whole_ms / 1000.0 : (total ? INFINITY : NAN);
+  if (std::isinf(rps)) fprintf(stderr, "RPS    : inf M\n");
+  else if (std::isnan(rps)) fprintf(stderr, "RPS    : NaN M\n");
+  else fprintf(stderr, "RPS    : %.3f M\n", rps);
 }
 
 int fail(const char* what) {

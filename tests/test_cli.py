@@ -63,3 +63,40 @@ def test_cli_without_gpu_fails_loudly(tmp_path):
     r = _run(["reduce", "--", "1"], tmp_path)
     assert r.returncode == 101
     assert "error" in r.stderr and "CUDA" in r.stderr
+
+
+GPU_RUNS = [c for c in RUNS if "not found" not in c["expect"]]
+STATS = [r"RWTS   : +[\d_]+", r"- ANNI : +[\d_]+", r"- COMM : +[\d_]+", r"- ERAS : +[\d_]+", r"- DREF : +[\d_]+",
+         r"- OPER : +[\d_]+", r"TIME   : \d+\.\d{3}(s|ms|µs|ns)", r"RPS    : (\d+\.\d{3}|inf|NaN) M"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", GPU_RUNS, ids=[" ".join(c["args"]) for c in GPU_RUNS])
+def test_cli_on_gpu_prints_reference_outputs(case, tmp_path):
+    """`hvm64 run` / `hvm64 reduce` reduce on the GPU and print the reference
+    CLI's normal forms (tests/cli.rs:40-131), and with -s the statistics block
+    of src/main.rs:195-204 (RWTS and per-rule lines with the reference's
+    pretty numbers and widths, TIME as a Duration, RPS) once per expression;
+    the counts equal the oracle's for the same net."""
+    import re
+    from oracle import oracle
+    path = tmp_path / "arithmetic.hvm"
+    path.write_text(CASES["arithmetic"])
+    args = [str(path) if a == "{arithmetic}" else a for a in case["args"]]
+    cut = args.index("--") if "--" in args else len(args)
+    r = _run(args[:cut] + ["-s"] + args[cut:], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == case["expect"]
+    lines = r.stderr.strip().split("\n")
+    outs = case["expect"].split("\n")
+    assert len(lines) == 8 * len(outs), r.stderr
+    nets = _run(args[:cut] + ["--print-net"] + args[cut:], tmp_path).stdout.strip().split("\n")
+    book = CASES["arithmetic"] if "{arithmetic}" in case["args"] else ""
+    for k, net in enumerate(nets):
+        block = lines[8 * k:8 * k + 8]
+        for line, pat in zip(block, STATS):
+            assert re.fullmatch(pat, line), (line, pat)
+        _, want = oracle.run_expr(book, net)
+        got = [int(l.split(":")[1].replace("_", "")) for l in block[1:6]]
+        assert got == [want[x] for x in ("anni", "comm", "eras", "dref", "oper")]
+        assert int(block[0].split(":")[1].replace("_", "")) == sum(want.values())
