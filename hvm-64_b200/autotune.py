@@ -3,7 +3,9 @@
 The knobs trade against each other per workload: resident reducer blocks per
 SM (occupancy vs. shared memory per warp), allocator chunk size (bump-pointer
 traffic vs. nodes stranded in half-used chunks), the stack depth above which a
-warp donates work (load balance vs. queue traffic) and the queue capacity.
+warp donates work (the steal threshold: load balance vs. queue traffic), the
+queue capacity, and how many warps one net's work may spread over (warps per
+net: locality in one net's heap vs. parallelism).
 `autotune` runs a sample of the batch (the nets are independent, so a sample
 has the batch's mix) under candidate settings and keeps the fastest by device
 time, one knob at a time (coordinate descent from the defaults), so the search
@@ -15,12 +17,13 @@ import hvm64
 
 # Candidate values per knob; 0 is the library default.
 SPACE = {
-    "blocks_per_sm": (0, 6, 4),
-    "chunk_nodes": (0, 4096),
-    "donate_min": (0, 32, 128),
+    "blocks_per_sm": (0, 6, 5),
+    "chunk_nodes": (0, 64, 1024, 4096),
+    "donate_min": (0, 32, 128, 256),
     "queue_slots_log2": (0, 18, 22),
+    "max_warps_per_net": (0, 64, 512),
 }
-ORDER = ("blocks_per_sm", "chunk_nodes", "donate_min", "queue_slots_log2")
+ORDER = ("blocks_per_sm", "chunk_nodes", "donate_min", "queue_slots_log2", "max_warps_per_net")
 
 
 def coordinate_search(measure, space=SPACE, order=ORDER, rounds=1):

@@ -69,7 +69,7 @@ struct Ctrl {
   ull spin_limit;
   ull deadline;    // %globaltimer ns
   ull donate_min;
-  ull lane_budget;
+  ull max_warps;   // holders (warps + queued slots) per net beyond which no work is donated; 0: no cap
   ull q_mask;
   int error;
   int error_net;

@@ -694,7 +694,11 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_
       if (lane == 0) {
         long long h = ld_gpu64s(&C->hungry);
         long long queued = (long long)(ld_gpu(&C->q_tail) - ld_gpu(&C->q_head));
-        give = (h > 0 && queued < h) ? 2 : sp_high ? 1 : 0;
+        // a net already spread over max_warps holders (warps and queued
+        // slots) gets no more, except to relieve a full overflow stack
+        ull cap = C->max_warps;
+        bool spread = cap && (ull)ld_gpu64s(&g_P.nets[cur].pending) >= cap;
+        give = (h > 0 && queued < h && !spread) ? 2 : sp_high ? 1 : 0;
       }
       give = __shfl_sync(0xffffffffu, give, 0);
       if (give) {
@@ -981,7 +985,7 @@ struct Runner {
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
-    c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+    c.max_warps = t.max_warps_per_net;
     c.q_mask = (1ull << qlog2) - 1;
     c.deadline = ~0ull;  // the boot kernel's deadline; warps of the reducer keep their own
     host_ctrl = c;
@@ -1151,7 +1155,7 @@ struct Runner {
   float run_graph(const hvm64_tuning& t, unsigned qlog2, uint64_t timeout_ms, unsigned first, unsigned count) {
     size_t qn = size_t(1) << qlog2;
     const unsigned n = unsigned(progs.size());
-    std::vector<uint64_t> key = {t.blocks_per_sm, t.chunk_nodes, t.donate_min, qlog2, t.lane_budget, timeout_ms,
+    std::vector<uint64_t> key = {t.blocks_per_sm, t.chunk_nodes, t.donate_min, qlog2, t.max_warps_per_net, timeout_ms,
                                  first, count, uint64_t(heap.p), uint64_t(q.p), uint64_t(d_defs.p), uint64_t(spill.p),
                                  spill_cap, grid};
     for (auto p : progs) key.push_back(p);
@@ -1169,7 +1173,7 @@ struct Runner {
       c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
       c.spin_limit = 1ull << 24;
       c.donate_min = t.donate_min ? t.donate_min : 64;
-      c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+      c.max_warps = t.max_warps_per_net;
       c.q_mask = qn - 1;
       c.deadline = ~0ull;
       c.timeout_ns = timeout_ms * 1000000ull;
@@ -1418,7 +1422,7 @@ struct Server {
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 32;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
-    c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+    c.max_warps = t.max_warps_per_net;
     c.q_mask = qn - 1;
     c.deadline = ~0ull;
     // a server runs until stopped, or until its lifetime (timeout_ms) ends
@@ -1872,7 +1876,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   c.chunk_nodes = t.chunk_nodes ? std::min<uint32_t>(t.chunk_nodes, 64) : CHUNK_NODES;
   c.spin_limit = 1ull << 24;
   c.donate_min = t.donate_min ? t.donate_min : 64;
-  c.lane_budget = t.lane_budget ? t.lane_budget : 1;
+  c.max_warps = t.max_warps_per_net;
   c.q_mask = (1ull << QLOG2) - 1;
   c.deadline = ~0ull;
   c.timeout_ns = timeout_ms * 1000000ull;

@@ -63,7 +63,7 @@ class Rewrites(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("chunk_nodes", ctypes.c_uint32),
                 ("donate_min", ctypes.c_uint32), ("queue_slots_log2", ctypes.c_uint32),
-                ("lane_budget", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("max_warps_per_net", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("timeout_ms", ctypes.c_uint64)]
 
 

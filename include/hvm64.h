@@ -45,13 +45,13 @@ typedef struct hvm64_rewrites {
 } hvm64_rewrites;
 
 /* Device launch knobs (0 = default).  hvm-64_b200/autotune.py picks blocks_per_sm,
- * chunk_nodes, donate_min and queue_slots_log2 for a batch. */
+ * chunk_nodes, donate_min, queue_slots_log2 and max_warps_per_net for a batch. */
 typedef struct hvm64_tuning {
   uint32_t blocks_per_sm;    /* resident reducer blocks per SM (2 warps each; 0: as many as fit) */
   uint32_t chunk_nodes;      /* nodes a lane takes from the global bump at once */
-  uint32_t donate_min;       /* warp-stack depth above which a warp shares work */
+  uint32_t donate_min;       /* warp-stack depth above which a warp shares work (the steal threshold) */
   uint32_t queue_slots_log2; /* global redex-queue capacity, in 32-redex slots (0: 2^20) */
-  uint32_t lane_budget;      /* no effect in this version (kept for layout stability) */
+  uint32_t max_warps_per_net; /* warps (plus queued slots) one net's work may spread over (0: no cap) */
   uint32_t flags;            /* HVM64_TUNE_* bits */
   uint64_t timeout_ms;       /* run deadline; a longer run fails with TIMEOUT */
 } hvm64_tuning;
