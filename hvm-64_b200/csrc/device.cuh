@@ -96,7 +96,8 @@ struct Ctrl {
   int pad7;
   ull pad8[14];
   ull free_top;       // shared stack of free-node batches: batch head address | push count << 44
-  ull pad9[15];
+  ull reuse_mark;     // bump position from which free nodes are shared between warps
+  ull pad9[14];
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -340,8 +341,7 @@ struct WarpSmem {
   unsigned icache_def;        // Def index staged in icache (~0u: none)
   ull rw[NCOUNT];             // counters of the warp's current net
   unsigned cnt[NCOUNT * 32];  // per lane: counts of this step, [counter][lane] (folded into rw)
-  ull ovf[32];                // per lane: overflow free list (left word links; right word LOCK)
-  unsigned ovf_n[32];         // per lane: nodes added to `ovf` since it was last published
+  ull ovf[32];                // per lane: free list head | pushes since published << 48 (see free_list_push)
   ull fw[4 * 32];             // per lane: words freed alone by the current interaction
   ull bnext[32], bend[32];    // per lane: pre-LOCKed bump chunk [bnext, bend), node indices
   unsigned allocs[32];        // per lane: nodes allocated (for the DREF statistics)
@@ -364,7 +364,6 @@ struct WarpSmem {
 HVM_INL void lane_init(WarpSmem* W, unsigned ln) {
   for (int k = 0; k < NCOUNT; k++) W->cnt[k * 32 + ln] = 0;
   W->ovf[ln] = 0;
-  W->ovf_n[ln] = 0;
   for (int k = 0; k < 4; k++) W->fw[k * 32 + ln] = 0;
   W->bnext[ln] = W->bend[ln] = 0;
   W->allocs[ln] = 0;
@@ -418,21 +417,30 @@ HVM_COLD uint32_t binary_op(unsigned net, uint32_t a, uint32_t op, uint32_t b) {
 // driver ships the redex to shared work (the CUDA driver: a one-redex queue
 // slot, or HVM64_ERR_QUEUE when the queue is full -- it never waits).
 HVM_COLD void push_overflow(unsigned net, ull a, ull b);
-// Free nodes move between warps through one shared stack of batches: a
-// lane's list of reclaimed nodes (linked through their left words, right
-// words LOCK) is published whole once it holds OVF_FLUSH nodes, the batch's
-// head node linking the next batch through its right word; a lane whose own
-// lists are empty takes a batch before it takes fresh nodes from the bump
-// pointer.  The top word carries a push/pop count above the address bits, so
-// a pop whose batch was taken and republished meanwhile fails its CAS (ABA).
+// A lane's free list of reclaimed nodes is linked through their left words
+// (right words LOCK); the lane's head word holds the first node's address in
+// bits 0-47 and the number of nodes pushed since the list was last
+// published in bits 48-63.
+//
+// Free nodes move between warps through one shared stack of batches, once
+// the heap is past its reuse mark (Ctrl::reuse_mark; a batch run sets it at
+// half the heap, a server at 0): a lane's list is published whole once it
+// holds OVF_FLUSH nodes, the batch's head node linking the next batch through
+// its right word, and a lane whose list is empty takes a batch before it
+// takes fresh nodes from the bump pointer.  Below the mark, allocation stays
+// on the bump pointer and the lanes' own lists (no shared traffic).  The top
+// word carries a push/pop count above the address bits, so a pop whose
+// batch was taken and republished meanwhile fails its CAS (ABA).
 #ifndef HVM_OVF_FLUSH
 #define HVM_OVF_FLUSH 128
 #endif
 constexpr unsigned OVF_FLUSH = HVM_OVF_FLUSH;
 constexpr ull FT_ADDR = (1ull << 44) - 1;
 constexpr ull FT_TAG = 1ull << 44;
-HVM_COLD void free_publish(unsigned net, ull* ovf, unsigned* ovf_n) {
-  ull head = *ovf;
+constexpr ull OVF_ADDR = (1ull << 48) - 1;
+HVM_INL bool past_reuse_mark() { return ld_gpu(&g_P.ctrl->bump) >= g_P.ctrl->reuse_mark; }
+HVM_COLD void free_publish(unsigned net, ull* ovf) {
+  ull head = *ovf & OVF_ADDR;
   if (!head) return;
   ull* top = &g_P.ctrl->free_top;
   unsigned it = 0;
@@ -444,7 +452,6 @@ HVM_COLD void free_publish(unsigned net, ull* ovf, unsigned* ovf_n) {
     if (!run_spin(net, it)) return;  // lost CASes are other lanes' progress; still bounded
   }
   *ovf = 0;
-  *ovf_n = 0;
 }
 // Take one batch from the shared stack as the lane's list; false when empty.
 HVM_COLD bool free_take(unsigned net, ull* ovf) {
@@ -464,18 +471,17 @@ HVM_COLD bool free_take(unsigned net, ull* ovf) {
   }
   return false;
 }
-// Pop the lane's free list (or a shared batch) / take a new pre-LOCKed bump
-// chunk.
+// Pop the lane's free list (or, past the reuse mark, a shared batch) / take
+// a new pre-LOCKed bump chunk.
 struct Refill {
   ull node, bnext, bend;
 };
-HVM_COLD Refill alloc_refill(unsigned net, ull* ovf, unsigned* ovf_n) {
-  if (*ovf != 0 || free_take(net, ovf)) {
-    ull a = *ovf;
-    *ovf = ld_gpu(heap_at(net, a));
+HVM_COLD Refill alloc_refill(unsigned net, ull* ovf) {
+  if ((*ovf & OVF_ADDR) != 0 || (past_reuse_mark() && free_take(net, ovf))) {
+    ull a = *ovf & OVF_ADDR, n = *ovf >> 48;
+    *ovf = (ld_gpu(heap_at(net, a)) & OVF_ADDR) | ((n ? n - 1 : 0) << 48);
     st_gpu(heap_at(net, a), P_LOCK);
     mem_fence();
-    if (*ovf_n) --*ovf_n;
     return {a, 0, 0};
   }
   ull n = g_P.ctrl->chunk_nodes;
@@ -489,10 +495,11 @@ HVM_COLD Refill alloc_refill(unsigned net, ull* ovf, unsigned* ovf_n) {
   return {s << 4, s + 1, s + n};
 }
 // A reclaimed node (both words LOCK) onto a lane's free list.
-HVM_INL void free_list_push(unsigned net, ull* ovf, unsigned* ovf_n, ull node) {
-  st_gpu(heap_at(net, node), *ovf);
-  *ovf = node;
-  if (++*ovf_n >= OVF_FLUSH) free_publish(net, ovf, ovf_n);
+HVM_INL void free_list_push(unsigned net, ull* ovf, ull node) {
+  ull n = (*ovf >> 48) + 1;
+  st_gpu(heap_at(net, node), *ovf & OVF_ADDR);
+  *ovf = node | (n < 0xFFFF ? n << 48 : 0xFFFFull << 48);
+  if (n >= OVF_FLUSH && past_reuse_mark()) free_publish(net, ovf);
 }
 
 // ---- the runtime proper ------------------------------------------------------
@@ -571,11 +578,11 @@ HVM_COLD void recycle(const Ctx& c, ull node) {
   if (k < c.W->pool_cap) {
     c.W->freed[k] = node;
   } else {
-    free_list_push(c.net, &LS(ovf), &LS(ovf_n), node);  // right word already LOCK
+    free_list_push(c.net, &LS(ovf), node);  // right word already LOCK
   }
 }
 HVM_COLD ull alloc_slow(const Ctx& c) {
-  Refill r = alloc_refill(c.net, &LS(ovf), &LS(ovf_n));
+  Refill r = alloc_refill(c.net, &LS(ovf));
   if (r.bend) {
     LS(bnext) = r.bnext;
     LS(bend) = r.bend;
@@ -737,8 +744,14 @@ HVM_COLD void half_link_wire_port(const Ctx& c, ull ap, ull aw, ull bp) {
 }
 HVM_COLD void link_wire_wire(const Ctx& c, ull aw, ull bw) {
   PROF_RULE(9)
-  ull ap = lock_target(c, aw);
-  ull bp = lock_target(c, bw);
+  // Both words belong to nodes this interaction consumes, so no other lane
+  // takes them: the two exchanges go out together (one round trip instead of
+  // two) and give the values the reference's take-one-then-the-other does; a
+  // word its creator has not written yet (LOCK) is waited for after both.
+  ull ap = hswap(c, aw, P_LOCK);
+  ull bp = hswap(c, bw, P_LOCK);
+  if (ap == P_LOCK) ap = relock(c.net, aw);
+  if (bp == P_LOCK) bp = relock(c.net, bw);
   if (principal(ap) && principal(bp)) {
     half_free(c, aw);
     half_free(c, bw);

@@ -240,13 +240,13 @@ __device__ __noinline__ void serve_release(WarpSmem& W, unsigned slot, ull root)
     visit(l);
     visit(r);
     st_gpu(heap_at(slot, a | 8), P_LOCK);
-    free_list_push(slot, &W.ovf[0], &W.ovf_n[0], a);
+    free_list_push(slot, &W.ovf[0], a);
   }
   // the root node: its left word held the root wire, its right half was
   // freed when the root was allocated (runtime/src/net.rs:65-69)
   ull rn = root & ~8ull;
   st_gpu(heap_at(slot, rn | 8), P_LOCK);
-  free_list_push(slot, &W.ovf[0], &W.ovf_n[0], rn);
+  free_list_push(slot, &W.ovf[0], rn);
   mem_fence();
 }
 
@@ -674,7 +674,7 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_
       for (int i = int(lane); i < mv; i += 32) W.pool[pn + i] = W.freed[i];
       for (int i = mv + int(lane); i < fn; i += 32) {
         // pool full: the rest goes to this lane's overflow list
-        free_list_push(unsigned(cur), &W.ovf[lane], &W.ovf_n[lane], W.freed[i]);
+        free_list_push(unsigned(cur), &W.ovf[lane], W.freed[i]);
       }
       __syncwarp();
       if (lane == 0) {
@@ -981,6 +981,7 @@ struct Runner {
     dev::Ctrl c{};
     c.bump = bump;  // node 0 is reserved
     c.heap_nodes = heap_bytes / 16;
+    c.reuse_mark = c.heap_nodes / 2;  // free nodes are shared between warps once half the heap is used
     c.heap_bytes = heap_bytes;
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
     c.spin_limit = 1ull << 24;
@@ -1169,6 +1170,7 @@ struct Runner {
       dev::Ctrl c{};
       c.bump = 1;
       c.heap_nodes = heap_bytes / 16;
+      c.reuse_mark = c.heap_nodes / 2;  // free nodes are shared between warps once half the heap is used
       c.heap_bytes = heap_bytes;
       c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 256;
       c.spin_limit = 1ull << 24;
@@ -1418,8 +1420,10 @@ struct Server {
     c.heap_nodes = heap_bytes / 16;
     c.heap_bytes = heap_bytes;
     // small allocator chunks: a server's heap is shared by requests for its
-    // whole life, so nodes stranded in part-used chunks count against it
+    // whole life, so nodes stranded in part-used chunks count against it; and
+    // free nodes are shared between warps from the start
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 32;
+    c.reuse_mark = 0;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
     c.max_warps = t.max_warps_per_net;
@@ -1872,6 +1876,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   dev::Ctrl c{};
   c.bump = 1;
   c.heap_nodes = HEAP_BYTES / 16;
+  c.reuse_mark = c.heap_nodes / 2;
   c.heap_bytes = HEAP_BYTES;
   c.chunk_nodes = t.chunk_nodes ? std::min<uint32_t>(t.chunk_nodes, 64) : CHUNK_NODES;
   c.spin_limit = 1ull << 24;

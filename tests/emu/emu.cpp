@@ -142,7 +142,7 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsig
     int pn = std::max(W->pool_n, 0), fn = std::min(W->freed_n, POOL), mv = std::min(fn, POOL - pn);
     for (int k = 0; k < mv; k++) W->pool[pn + k] = W->freed[k];
     for (int k = mv; k < fn; k++) {
-      free_list_push(c.net, &W->ovf[0], &W->ovf_n[0], W->freed[k]);
+      free_list_push(c.net, &W->ovf[0], W->freed[k]);
     }
     W->pool_n = pn + mv;
     W->freed_n = 0;
@@ -192,6 +192,7 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     E.C.heap_nodes = heap_bytes / 16;
     E.C.heap_bytes = heap_bytes;
     E.C.chunk_nodes = chunk;
+    E.C.reuse_mark = 0;  // free nodes shared between threads from the start
     E.C.spin_limit = 1ull << 26;
     E.C.deadline = globaltimer() + 120ull * 1000000000ull;
     E.P.heap = E.heap.data();

@@ -128,7 +128,7 @@ def test_server_long_run_heap_stays_bounded():
     hvm64 = _hvm()
     reqs = [("sort", 12, j) for j in range(8)]
     book = hvm64.Book.from_str(W.serving_book(reqs))
-    sv = hvm64.Server(book, slots=32, out_pairs=1 << 16, heap_bytes=4 << 30,
+    sv = hvm64.Server(book, slots=32, out_pairs=1 << 18, heap_bytes=4 << 30,
                       tuning=hvm64.Tuning(timeout_ms=300000))
     try:
         owner, done, submitted, high_60 = {}, 0, 0, None
