@@ -273,7 +273,7 @@ def serve_leg(args, hvm64):
         # continuous batching, in real time; the server's lifetime ends soon
         # after the last arrival's wait
         life_ms = int(1000 * (arr[-1] + args.serve_wait_s)) + 5000
-        sv = hvm64.Server(book, slots=args.serve_slots, out_pairs=1 << 18, heap_bytes=16 << 30,
+        sv = hvm64.Server(book, slots=args.serve_slots, out_pairs=1 << 19, heap_bytes=16 << 30,
                           tuning=hvm64.Tuning(timeout_ms=life_ms))
         lat, owner, i = [], {}, 0
         t_start = time.perf_counter()

@@ -152,6 +152,7 @@ struct Params {
   // spill[2 * spill_cap * g ...] (spill_cap redexes); null: none
   unsigned spill_cap;
   ull* spill;
+  unsigned ovf_flush;           // free-list length at which a lane publishes it (see free_list_push)
   // serving (all zero for a batch run)
   unsigned serve;
   const ServeReq* req;         // device ring of req_cap requests
@@ -425,7 +426,8 @@ HVM_COLD void push_overflow(unsigned net, ull a, ull b);
 // Free nodes move between warps through one shared stack of batches, once
 // the heap is past its reuse mark (Ctrl::reuse_mark; a batch run sets it at
 // half the heap, a server at 0): a lane's list is published whole once it
-// holds OVF_FLUSH nodes, the batch's head node linking the next batch through
+// holds Params::ovf_flush nodes (OVF_FLUSH for a batch, 32 for a server, which
+// keeps fewer nodes stranded per lane), the batch's head node linking the next batch through
 // its right word, and a lane whose list is empty takes a batch before it
 // takes fresh nodes from the bump pointer.  Below the mark, allocation stays
 // on the bump pointer and the lanes' own lists (no shared traffic).  The top
@@ -434,7 +436,7 @@ HVM_COLD void push_overflow(unsigned net, ull a, ull b);
 #ifndef HVM_OVF_FLUSH
 #define HVM_OVF_FLUSH 128
 #endif
-constexpr unsigned OVF_FLUSH = HVM_OVF_FLUSH;
+constexpr unsigned OVF_FLUSH = HVM_OVF_FLUSH;  // batch runs (a server publishes after 32)
 constexpr ull FT_ADDR = (1ull << 44) - 1;
 constexpr ull FT_TAG = 1ull << 44;
 constexpr ull OVF_ADDR = (1ull << 48) - 1;
@@ -499,7 +501,7 @@ HVM_INL void free_list_push(unsigned net, ull* ovf, ull node) {
   ull n = (*ovf >> 48) + 1;
   st_gpu(heap_at(net, node), *ovf & OVF_ADDR);
   *ovf = node | (n < 0xFFFF ? n << 48 : 0xFFFFull << 48);
-  if (n >= OVF_FLUSH && past_reuse_mark()) free_publish(net, ovf);
+  if (n >= g_P.ovf_flush && past_reuse_mark()) free_publish(net, ovf);
 }
 
 // ---- the runtime proper ------------------------------------------------------

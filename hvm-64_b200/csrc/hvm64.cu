@@ -954,6 +954,7 @@ struct Runner {
     p.ndefs = unsigned(book.defs.size());
     p.spill = spill.p;
     p.spill_cap = spill_cap;
+    p.ovf_flush = dev::OVF_FLUSH;
     return p;
   }
 
@@ -1339,6 +1340,10 @@ void Runner::set_deadline(cudaStream_t st, uint64_t timeout_ms) {
 // output and posts a completion record, both in mapped host memory, which the
 // host polls.  Slots bound the nets in flight; the heap is shared and only
 // grows (normal forms stay until the server is freed).
+// A server's lanes publish their free lists after this many nodes: fewer
+// nodes stay stranded per lane over a server's long life.
+constexpr unsigned SERVE_OVF_FLUSH = 32;
+
 struct Server {
   Book book;
   int device = 0, sms = 148;
@@ -1456,7 +1461,8 @@ struct Server {
     // Node budget for admission: the heap minus what the allocator can hold
     // back while nothing is live (each lane's part-used chunk and unpublished
     // free list, each warp's reuse pool).
-    const uint64_t reserve = warps * 32 * (c.chunk_nodes + dev::OVF_FLUSH) + warps * dev::POOL;
+    p.ovf_flush = SERVE_OVF_FLUSH;
+    const uint64_t reserve = warps * 32 * (c.chunk_nodes + SERVE_OVF_FLUSH) + warps * dev::POOL;
     if (heap_bytes / 16 <= 2 * reserve)
       throw Error(HVM64_ERR_BAD_INPUT, "heap_bytes too small for a server: its allocator may hold back " +
                                            std::to_string(reserve) + " nodes; give it at least " +
@@ -1905,6 +1911,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   p.ndefs = unsigned(book.defs.size());
   p.spill = reinterpret_cast<dev::ull*>(base + OFF_SPILL);
   p.spill_cap = SPILL;
+  p.ovf_flush = dev::OVF_FLUSH;
   hvm64_tuning tg = t;
   if (tg.blocks_per_sm == 0 || tg.blocks_per_sm > 4) tg.blocks_per_sm = 4;
   unsigned grid = std::min(unsigned(sms * reducer_blocks_per_sm(tg)), MAX_WARPS / unsigned(dev::WARPS));

@@ -204,6 +204,7 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     E.P.instrs = book.instrs.data();
     E.P.labbits = reinterpret_cast<const ull*>(book.labbits.data());
     E.P.ndefs = unsigned(book.defs.size());
+    E.P.ovf_flush = OVF_FLUSH;
     g_P = E.P;
     // boot (the boot kernel's steps, one thread)
     g_emu = &E;
