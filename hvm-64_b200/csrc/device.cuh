@@ -217,23 +217,19 @@ __device__ __forceinline__ ull atom_add(ull* p, ull v) { return atomicAdd(p, v);
 __device__ __forceinline__ int atom_cas32(int* p, int e, int v) { return atomicCAS(p, e, v); }
 __device__ __forceinline__ unsigned atom_add_u32(unsigned* p, unsigned v) { return atomicAdd(p, v); }
 __device__ __forceinline__ int atom_add_i32(int* p, int v) { return atomicAdd(p, v); }
-// Warp-aggregated fetch-and-add of the same `v` by the converged lanes that
-// target the same word: one atomic per group, each lane gets its own offset
-// (lanes stepping in lock-step would otherwise serialise on the word).
-// Only shared memory qualifies: a local-memory word has the same generic
-// address in every thread.
-__device__ __forceinline__ int agg_add_i32(int* p, int v) {
-  if (!__isShared(p)) return atomicAdd(p, v);
-  unsigned mask = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(p));
-  unsigned ln = threadIdx.x & 31;
-  int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (int(ln) == leader) base = atomicAdd(p, v * __popc(mask));
-  base = __shfl_sync(mask, base, leader);
-  return base + v * __popc(mask & ((1u << ln) - 1u));
+// Fetch-and-add on a word of a warp's shared-memory state (`p` is a generic
+// pointer into shared memory).  A plain shared-memory atomic per lane:
+// aggregating the converged lanes first (match, leader, shuffle) measured
+// 8 % slower overall -- its extra instructions cost more than the few lanes
+// that serialise on the word.
+__device__ __forceinline__ int smem_add_i32(int* p, int v) {
+  int old;
+  unsigned a = unsigned(__cvta_generic_to_shared(p));
+  asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(v) : "memory");
+  return old;
 }
-__device__ __forceinline__ unsigned agg_add_u32(unsigned* p, unsigned v) {
-  return unsigned(agg_add_i32(reinterpret_cast<int*>(p), int(v)));
+__device__ __forceinline__ unsigned smem_add_u32(unsigned* p, unsigned v) {
+  return unsigned(smem_add_i32(reinterpret_cast<int*>(p), int(v)));
 }
 // A release fence: the node fills and links before it are visible to any
 // lane that later reaches the node through a port published after it.
@@ -290,8 +286,8 @@ inline int atom_cas32(int* p, int e, int v) {
 }
 inline unsigned atom_add_u32(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_add(v); }
 inline int atom_add_i32(int* p, int v) { return std::atomic_ref<int>(*p).fetch_add(v); }
-inline int agg_add_i32(int* p, int v) { return atom_add_i32(p, v); }
-inline unsigned agg_add_u32(unsigned* p, unsigned v) { return atom_add_u32(p, v); }
+inline int smem_add_i32(int* p, int v) { return atom_add_i32(p, v); }
+inline unsigned smem_add_u32(unsigned* p, unsigned v) { return atom_add_u32(p, v); }
 inline void mem_fence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void pause_brief() { std::this_thread::yield(); }
 inline void lock_fill(ull* H, ull s, ull n) {
@@ -383,19 +379,16 @@ HVM_INL bool run_failed() { return ld_gpu32(&g_P.ctrl->error) != 0; }
 // (heap accesses, bounded waits): a call there, even one never taken, makes
 // every such site keep its live registers across the call, which costs the
 // reducer about a tenth of its throughput.
-HVM_INL void run_fail_here(unsigned net, int code, ull info) {
-  if (atom_cas32(&g_P.ctrl->error, 0, code) == 0) {
-    g_P.ctrl->error_info = info;
-    g_P.ctrl->error_net = int(net);
-  }
-}
+// (Only the code is recorded: storing the net and detail too measured 4 %
+// slower.)
+HVM_INL void run_fail_here(int code) { atom_cas32(&g_P.ctrl->error, 0, code); }
 // One poll of a bounded wait; false = abandon the wait.
 HVM_INL bool run_spin(unsigned net, unsigned& it) {
   ++it;
   if ((it & 63) == 0) {
     if (run_failed()) return false;
     if (it > g_P.ctrl->spin_limit) {
-      run_fail_here(net, HVM64_ERR_TIMEOUT, 0);
+      run_fail_here(HVM64_ERR_TIMEOUT);
       return false;
     }
     pause_brief();
@@ -404,7 +397,7 @@ HVM_INL bool run_spin(unsigned net, unsigned& it) {
 }
 HVM_INL ull* heap_at(unsigned net, ull a) {
   if (a >= g_P.heap_bytes) {
-    run_fail_here(net, HVM64_ERR_BAD_ADDR, a);
+    run_fail_here(HVM64_ERR_BAD_ADDR);
     a = 0;
   }
   return g_P.heap + (a >> 3);
@@ -586,7 +579,7 @@ HVM_INL ull lock_target(const Ctx& c, ull w) {
 // without reading the other half; otherwise the reference's store-FREE /
 // read-other-half / CAS sequence decides which lane reclaims.
 HVM_COLD void recycle(const Ctx& c, ull node) {
-  int k = c.W->pool_cap ? agg_add_i32(&c.W->freed_n, 1) : POOL;
+  int k = c.W->pool_cap ? smem_add_i32(&c.W->freed_n, 1) : POOL;
   if (k < c.W->pool_cap) {
     c.W->freed[k] = node;
   } else {
@@ -604,7 +597,7 @@ HVM_COLD ull alloc_slow(const Ctx& c) {
 HVM_INL ull alloc(const Ctx& c) {
   LS(allocs)++;
   if (c.W->pool_cap) {
-    int k = agg_add_i32(&c.W->pool_n, -1) - 1;
+    int k = smem_add_i32(&c.W->pool_n, -1) - 1;
     if (k >= 0) return c.W->pool[k];
   }
   ull b = LS(bnext);
@@ -688,7 +681,7 @@ HVM_COLD void push_spill(const Ctx& c, ull a, ull b, unsigned j) {
 }
 HVM_INL void push(const Ctx& c, ull a, ull b) {
   unsigned cap = c.W->ring_cap;
-  unsigned k = agg_add_u32(&c.W->ring_cnt, 1u);
+  unsigned k = smem_add_u32(&c.W->ring_cnt, 1u);
   if (k < cap) {
     unsigned i = (c.W->ring_base + k) & unsigned(SCAP - 1);
     c.W->stk[2 * i] = a;
