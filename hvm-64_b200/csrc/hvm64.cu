@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -202,9 +203,7 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
 // or writes its net's pairs at offs[i].  A net whose walk overflows the
 // stack gets count ~0u and is read back from a heap image instead.
 constexpr unsigned GATHER_STACK = 256;
-__global__ void gather_kernel(const __grid_constant__ Params P, unsigned first, unsigned n, unsigned* counts,
-                              const ull* offs, ull* out) {
-  load_params(P);
+__global__ void gather_kernel(unsigned first, unsigned n, unsigned* counts, const ull* offs, ull* out) {
   unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   i += first;
@@ -333,8 +332,7 @@ constexpr int QW = HVM_QW;  // selection window: 32 * QW newest redexes
 constexpr size_t SMEM_BYTES = sizeof(WarpSmem) * WARPS;
 static_assert(SMEM_BYTES <= 32 * 1024, "seven reducer blocks per SM must fit in shared memory");
 
-__global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_constant__ Params P) {
-  load_params(P);
+__global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
@@ -735,9 +733,7 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel(const __grid_
 // (Net::expand, runtime/src/net.rs:65-69).  Redexes collect in the warp's
 // stack (SCAP of them; more go out one per queue slot) and the warp
 // publishes them to the global queue in slots of up to 32.
-__global__ void __launch_bounds__(THREADS) boot_kernel(const __grid_constant__ Params P, unsigned first,
-                                                       unsigned count) {
-  load_params(P);
+__global__ void __launch_bounds__(THREADS) boot_kernel(unsigned first, unsigned count) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& W = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
@@ -881,6 +877,63 @@ unsigned boot_blocks(unsigned count, int sms) {
   return std::max(1u, std::min(b, unsigned(sms) * 8u));
 }
 
+// Runs on one device take turns: a run owns the device's constant-memory
+// launch parameters (dev::g_P) from their upload until its kernels finish.
+// A persistent reducer launch fills every SM, so runs of different handles
+// would not overlap much anyway.  A server holds its device's turn for its
+// whole life; another thread then waits (up to the given time) and the
+// server's own thread is refused rather than deadlocked.
+constexpr int MAX_DEVICES = 64;
+struct DeviceSlot {
+  std::mutex m;
+  std::condition_variable cv;
+  bool busy = false, server = false;
+  std::thread::id owner;
+};
+DeviceSlot g_turns[MAX_DEVICES];
+
+class DeviceTurn {
+ public:
+  DeviceTurn() = default;
+  DeviceTurn(int device, uint64_t wait_ms, bool server = false) { take(device, wait_ms, server); }
+  DeviceTurn(const DeviceTurn&) = delete;
+  DeviceTurn& operator=(const DeviceTurn&) = delete;
+  ~DeviceTurn() { release(); }
+  void take(int device, uint64_t wait_ms, bool server) {
+    if (device < 0 || device >= MAX_DEVICES) throw Error(HVM64_ERR_CUDA, "device index out of range");
+    DeviceSlot& d = g_turns[device];
+    std::unique_lock<std::mutex> lk(d.m);
+    if (d.busy && d.owner == std::this_thread::get_id())
+      throw Error(HVM64_ERR_BAD_INPUT, d.server ? "a server started by this thread holds the device: free it first"
+                                                : "the device is already in use by this thread");
+    if (!d.cv.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !d.busy; }))
+      throw Error(HVM64_ERR_TIMEOUT, "the device stayed in use by another run (a server holds its device until freed)");
+    d.busy = true;
+    d.server = server;
+    d.owner = std::this_thread::get_id();
+    dev_ = device;
+  }
+  void release() {
+    if (dev_ < 0) return;
+    DeviceSlot& d = g_turns[dev_];
+    {
+      std::lock_guard<std::mutex> lk(d.m);
+      d.busy = d.server = false;
+      d.owner = std::thread::id();
+    }
+    d.cv.notify_all();
+    dev_ = -1;
+  }
+
+ private:
+  int dev_ = -1;
+};
+
+// Uploads a run's launch parameters on its stream (inside its turn).
+void upload_params(const dev::Params& p, cudaStream_t st) {
+  CU(cudaMemcpyToSymbolAsync(dev::g_P, &p, sizeof p, 0, cudaMemcpyHostToDevice, st));
+}
+
 }  // namespace
 
 // Default redex-queue capacity: 2^20 slots (570 MB).  A warp whose stack is
@@ -971,10 +1024,10 @@ struct Runner {
   // Reduce nets [first, first+count) (the rest stay untouched); the grid is
   // prepared (prepare_grid) for this tuning.
   void launch(unsigned first, unsigned count, cudaStream_t st) {
-    dev::Params p = params();
-    dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, st>>>(p, first, count);
+    upload_params(params(), st);
+    dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, st>>>(first, count);
     CU(cudaGetLastError());
-    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>(p);
+    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>();
     CU(cudaGetLastError());
   }
 
@@ -1006,6 +1059,7 @@ struct Runner {
     count = unsigned(std::min<uint64_t>(count, progs.size() - first));
     run_first = first;
     run_count = count;
+    DeviceTurn turn(device, t.timeout_ms ? t.timeout_ms : 120000);
     unsigned qlog2 = t.queue_slots_log2 ? t.queue_slots_log2 : DEFAULT_QLOG2;
     if (qlog2 < 4 || qlog2 > 24) throw Error(HVM64_ERR_BAD_INPUT, "queue_slots_log2 out of range");
     h2d = d2h = 0;
@@ -1140,12 +1194,15 @@ struct Runner {
   std::vector<uint64_t> gkey;
   dev::Ctrl* pin_ctrl = nullptr;
   dev::NetState* pin_nets = nullptr;
+  dev::Params* pin_params = nullptr;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
     if (pin_ctrl) cudaFreeHost(pin_ctrl);
     if (pin_nets) cudaFreeHost(pin_nets);
+    if (pin_params) cudaFreeHost(pin_params);
+    pin_params = nullptr;
     pin_ctrl = nullptr;
     pin_nets = nullptr;
   }
@@ -1181,7 +1238,8 @@ struct Runner {
       c.deadline = ~0ull;
       c.timeout_ns = timeout_ms * 1000000ull;
       *pin_ctrl = c;
-      const dev::Params p = params();
+      CU(cudaHostAlloc(reinterpret_cast<void**>(&pin_params), sizeof(dev::Params), cudaHostAllocDefault));
+      *pin_params = params();
       CU(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaSuccess;
@@ -1194,9 +1252,10 @@ struct Runner {
       step(cudaGetLastError());
       dev::set_deadline_kernel<<<1, 1, 0, gs>>>(ctrl.p, c.timeout_ns);
       step(cudaGetLastError());
-      dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, gs>>>(p, first, count);
+      step(cudaMemcpyToSymbolAsync(dev::g_P, pin_params, sizeof(dev::Params), 0, cudaMemcpyHostToDevice, gs));
+      dev::boot_kernel<<<boot_blocks(count, sms), dev::THREADS, dev::SMEM_BYTES, gs>>>(first, count);
       step(cudaGetLastError());
-      dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, gs>>>(p);
+      dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, gs>>>();
       step(cudaGetLastError());
       cudaError_t ec = cudaStreamEndCapture(gs, &g);
       if (e == cudaSuccess) e = ec;
@@ -1257,12 +1316,13 @@ struct Runner {
   // Gathers the normal forms of the last run's nets (device-side walk).
   void gather_all() {
     const unsigned n = unsigned(progs.size()), first = run_first, cnt = run_count;
-    const dev::Params p = params();
+    DeviceTurn turn(device, 600000);
+    upload_params(params(), 0);
     d_gcount.alloc(n);
     unsigned blocks = (cnt + 127) / 128;
     gcount.assign(n, ~0u);
     if (cnt) CU(cudaMemcpy(d_gcount.p, gcount.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
-    if (cnt) dev::gather_kernel<<<blocks, 128>>>(p, first, cnt, d_gcount.p, nullptr, nullptr);
+    if (cnt) dev::gather_kernel<<<blocks, 128>>>(first, cnt, d_gcount.p, nullptr, nullptr);
     CU(cudaGetLastError());
     CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     for (unsigned i = 0; i < n; i++)
@@ -1276,7 +1336,7 @@ struct Runner {
     d_goff.alloc(n);
     CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
     d_gpairs.alloc(2 * tot);
-    if (cnt) dev::gather_kernel<<<blocks, 128>>>(p, first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
+    if (cnt) dev::gather_kernel<<<blocks, 128>>>(first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
     CU(cudaGetLastError());
     gpairs.resize(2 * tot);
     if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
@@ -1370,6 +1430,7 @@ struct Server {
   std::vector<uint64_t> slot_nodes;   // the node budget each slot's request holds
   std::vector<unsigned> free_slots;
   uint64_t budget_nodes = 0, reserved_nodes = 0;
+  DeviceTurn turn;  // the device's launch parameters are this server's while it runs
 
   ~Server() { shutdown(); }
 
@@ -1472,8 +1533,10 @@ struct Server {
     p.spill_cap = spill_cap_for(heap_bytes, warps);
     spill.alloc(2 * size_t(p.spill_cap) * warps);
     p.spill = spill.p;
-    CU(cudaStreamSynchronize(ks));  // tables in place before the reducer starts
-    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, ks>>>(p);
+    turn.take(device, t.timeout_ms ? t.timeout_ms : 120000, true);  // held until shutdown
+    upload_params(p, ks);
+    CU(cudaStreamSynchronize(ks));  // tables and parameters in place before the reducer starts
+    dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, ks>>>();
     CU(cudaGetLastError());
     running = true;
     slot_ticket.assign(nslots, 0);
@@ -1576,6 +1639,7 @@ struct Server {
       cudaStreamSynchronize(ks);
       running = false;
     }
+    turn.release();
     if (ks) cudaStreamDestroy(ks);
     if (cs) cudaStreamDestroy(cs);
     ks = cs = nullptr;
@@ -1843,6 +1907,8 @@ unsigned char* scratch_here(int device) {
   return g_dev_scratch[device];
 }
 
+uint64_t timeout_ms_of(const hvm64_tuning& t) { return t.timeout_ms ? t.timeout_ms : 120000; }
+
 std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm64_rewrites* out) {
   hvm64_tuning t{};
   if (tp) t = *tp;
@@ -1862,6 +1928,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   CU(cudaGetDevice(&device));
   CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   unsigned char* base = scratch_here(device);
+  DeviceTurn turn(device, timeout_ms_of(t));
   dev::Ctrl* ctrl = reinterpret_cast<dev::Ctrl*>(base + OFF_CTRL);
   dev::NetState* ns = reinterpret_cast<dev::NetState*>(base + OFF_NET);
   dev::Slot* q = reinterpret_cast<dev::Slot*>(base + OFF_QUEUE);
@@ -1915,9 +1982,10 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   hvm64_tuning tg = t;
   if (tg.blocks_per_sm == 0 || tg.blocks_per_sm > 4) tg.blocks_per_sm = 4;
   unsigned grid = std::min(unsigned(sms * reducer_blocks_per_sm(tg)), MAX_WARPS / unsigned(dev::WARPS));
-  dev::boot_kernel<<<1, dev::THREADS, dev::SMEM_BYTES, st>>>(p, 0, 1);
+  upload_params(p, st);
+  dev::boot_kernel<<<1, dev::THREADS, dev::SMEM_BYTES, st>>>(0, 1);
   CU(cudaGetLastError());
-  dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>(p);
+  dev::reduce_kernel<<<grid, dev::THREADS, dev::SMEM_BYTES, st>>>();
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(st));
 

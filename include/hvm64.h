@@ -11,8 +11,13 @@
  *    message of the last failure on the calling thread.
  *  - Handles are owned by the caller and released with the *_free calls.
  *    One handle is used by one host thread at a time (the reference's
- *    `&mut Net`); different handles may be used from different threads at
- *    once, on one device or several (each launch carries its own parameters).
+ *    `&mut Net`).  Different handles may be used from different threads:
+ *    calls that run kernels on one device take turns (a run holds the
+ *    device's launch parameters until its kernels finish; a persistent
+ *    launch fills every SM, so runs would not overlap anyway).  A call that
+ *    waits longer than its tuning's timeout_ms for its turn returns
+ *    HVM64_ERR_TIMEOUT.  A running server holds its device until it is freed:
+ *    calls from its own thread on that device return HVM64_ERR_BAD_INPUT.
  *  - A net's heap, redex queue and Book tables live in device memory behind
  *    the handle; buffers in these signatures are host memory.
  *  - No torch or CUDA types appear here; the library picks the current CUDA
@@ -147,8 +152,8 @@ int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
  * convention) and frees its slot.  hvm64_server_free stops the reducer at
  * once; requests still running are abandoned.
  *
- * A server's reducer occupies every SM while it runs, so other entry points
- * on that device wait for SMs (they stay correct).  An error in any request
+ * A server holds its device while it runs: calls of other threads on that
+ * device wait for it to be freed (see the conventions above).  An error in any request
  * (OOM, DIV0, BAD_PAIR, ...) stops the whole server; poll then returns it.
  * A server lives at most tuning->timeout_ms (default 10 minutes), then stops
  * with HVM64_ERR_TIMEOUT. */
@@ -198,10 +203,11 @@ void hvm64_server_free(hvm64_server* server);
  * The first call on a device looks up the array's device address (with that
  * device current); make that first call before any stream capture.  Every call
  * on a device shares the array and starts by resetting the parts a run reads
- * (control block, net record, queue, Book tables), so two of these calls that
- * overlap on the GPU (from two host threads) race and must be serialised by
- * the caller; other entry points use memory of their own and do not race with
- * it.  Outputs: `out` (nullable) receives the Rewrites; the normal form is
+ * (control block, net record, queue, Book tables), so two calls that overlapped
+ * on the GPU would race on it; calls on one device take turns like every other
+ * run (each call holds the device until its kernels finish and its results
+ * are copied back), so calls from different host threads are serialised.
+ * Outputs: `out` (nullable) receives the Rewrites; the normal form is
  * written as hvm64_net_readback writes it (buf/cap/len). */
 int hvm64_net_normal_noalloc(const hvm64_book* book, const char* def_name, const hvm64_tuning* tuning,
                              hvm64_rewrites* out, char* buf, size_t cap, size_t* len);

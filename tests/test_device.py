@@ -273,9 +273,9 @@ def test_bitonic_depth20_full_size():
 @pytest.mark.gpu
 def test_concurrent_handles_two_threads():
     """Two nets on one device, reduced from two host threads at the same
-    time (ctypes releases the GIL around each C call): each run gets its own
-    launch parameters, so both normal forms and all counts equal the
-    oracle's, on every round."""
+    time (ctypes releases the GIL around each C call): the runs take turns on
+    the device's launch parameters, so both normal forms and all counts equal
+    the oracle's, on every round."""
     import threading
     import workloads as W
     hvm64, oracle = _hvm(), _oracle()

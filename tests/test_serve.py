@@ -193,3 +193,23 @@ def test_server_admits_by_node_budget():
         assert sv.budget()["reserved"] == 0
     finally:
         sv.close()
+
+
+@pytest.mark.gpu
+def test_server_holds_its_device():
+    """A running server holds its device's launch parameters: a reduction
+    started from the server's own thread on that device is refused (it could
+    only wait for itself) instead of hanging, and works once the server is
+    freed."""
+    hvm64 = _hvm()
+    src = "@main = x & 3 ~ $([*] $(5 x))\n"
+    sv = hvm64.Server(hvm64.Book.from_str(src), slots=4, out_pairs=1 << 10, heap_bytes=1 << 30,
+                      tuning=hvm64.Tuning(timeout_ms=60000))
+    try:
+        with pytest.raises(hvm64.HvmError) as e:
+            hvm64.run_book(src, heap_bytes=1 << 24)
+        assert e.value.code == hvm64.ERR_BAD_INPUT and "server" in str(e.value)
+    finally:
+        sv.close()
+    got, _ = hvm64.run_book(src, heap_bytes=1 << 24)
+    assert got == "15"
