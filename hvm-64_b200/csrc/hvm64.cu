@@ -661,7 +661,11 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
       __syncwarp();
       if (lane == 0) W.sp_n += spilled;
     }
-    fold_counts(W);
+    // The lanes' counters fold into the warp's when it lets its net go (and
+    // every 256 steps, which bounds a lane's 32-bit counts); folding every
+    // step measured 4 % slower.
+    if ((step & 255) == 0) fold_counts(W);
+    else __syncwarp();
     // Nodes reclaimed in this step become allocatable after a fence.
     mem_fence();
     __syncwarp();
