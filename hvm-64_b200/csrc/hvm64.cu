@@ -169,6 +169,8 @@ __device__ __forceinline__ void fold_counts(WarpSmem& W) {
   __syncwarp();
 }
 
+__device__ __noinline__ void fold_counts_cold(WarpSmem& W) { fold_counts(W); }
+
 // Flush the warp's counters into its net (one atomic per counter).
 __device__ void flush_counters(WarpSmem& W, int cur) {
   const unsigned lane = threadIdx.x & 31;
@@ -639,7 +641,9 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
     if (lane < n) {
       long long l0 = clock64();
       interact(c, W.sel[2 * lane], W.sel[2 * lane + 1]);
-      settle(c);
+      // (a call to settle only when the lane freed a word alone: measured
+      // 5 % faster than calling it to find out)
+      if (W.fw[lane] | W.fw[32 + lane] | W.fw[64 + lane] | W.fw[96 + lane]) settle(c);
       mine = unsigned(min(clock64() - l0, 0x7fffffffll));
     }
     __syncwarp();
@@ -661,10 +665,10 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
       __syncwarp();
       if (lane == 0) W.sp_n += spilled;
     }
-    // The lanes' counters fold into the warp's when it lets its net go (and
-    // every 256 steps, which bounds a lane's 32-bit counts); folding every
-    // step measured 4 % slower.
-    if ((step & 255) == 0) fold_counts(W);
+    // The lanes' counters fold into the warp's when it lets its net go, and
+    // out of line every 4096 steps (which bounds a lane's 32-bit counts);
+    // folding every step measured 4 % slower.
+    if ((step & 4095) == 0) fold_counts_cold(W);
     else __syncwarp();
     // Nodes reclaimed in this step become allocatable after a fence.
     mem_fence();
