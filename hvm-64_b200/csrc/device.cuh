@@ -153,6 +153,9 @@ struct Params {
   unsigned spill_cap;
   ull* spill;
   unsigned ovf_flush;           // free-list length at which a lane publishes it (see free_list_push)
+  // register files of Def calls needing more than LOCAL_REGS registers:
+  // warp g owns bigregs[32 * MAX_REGS * g ...], [register][lane]; null: none
+  ull* bigregs;
   // serving (all zero for a batch run)
   unsigned serve;
   const ServeReq* req;         // device ring of req_cap requests
@@ -337,6 +340,7 @@ struct WarpSmem {
   unsigned ring_base;         // this step's pushes go to stack slots ring_base + k ...
   unsigned ring_cap;          // ... for k < ring_cap; push k >= ring_cap goes to the overflow stack
   ull* sp;                    // this warp's overflow stack in HBM (null: none; pushes go to the queue)
+  ull* bigregs;               // this warp's register files for Defs above LOCAL_REGS (null: none)
   unsigned sp_n, sp_cap;      // redexes in it between steps, and its capacity
   int pool_cap;               // 0: no reuse pool (reclaimed nodes go to `ovf`)
 #ifdef HVM_PROFILE_OPS
@@ -1032,8 +1036,13 @@ HVM_COLD void exec(const Ctx& c, const DevDef& d, ull t0, ull* R, unsigned strid
   }
 }
 HVM_COLD void exec_large(const Ctx& c, const DevDef& d, ull t0) {
-  ull R[MAX_REGS];
-  exec(c, d, t0, R, 1, g_P.instrs + d.ins_off);
+  if (d.nregs <= LOCAL_REGS) {
+    ull R[LOCAL_REGS];
+    return exec(c, d, t0, R, 1, g_P.instrs + d.ins_off);
+  }
+  // (the reference grows its register scratch to any Def, runtime/src/def.rs:221-223)
+  if (!c.W->bigregs || d.nregs > MAX_REGS) return run_fail(c.net, HVM64_ERR_BAD_INPUT, d.nregs);
+  exec(c, d, t0, c.W->bigregs + c.lane, 32, g_P.instrs + d.ins_off);
 }
 HVM_COLD void run_def(const Ctx& c, unsigned id, ull t0) {
   PROF_RULE(5)

@@ -654,20 +654,25 @@ static void emit(Book& book, const std::vector<RawInstr>& raw, uint32_t nregs, D
 }  // namespace
 
 // Encodes a Def's net into device instructions: in the reference's order,
-// or smaller-child-first when that order needs more than MAX_REGS registers.
+// or smaller-child-first when that order needs more than LOCAL_REGS
+// registers and the other does not (else the order needing fewer).
 static uint32_t encode_net(Book& book, const AstNet& net, DevDef& d) {
+  std::vector<RawInstr> best;
+  uint32_t best_regs = 0;
   for (int pass = 0; pass < 2; pass++) {
     Encoder e{book, {}, 1, {}};
     e.small_first = pass == 1;
     e.net(net, 0);
     if (!e.scope.empty()) throw Error(HVM64_ERR_BAD_INPUT, "unbound variables: " + e.scope.begin()->first);
     uint32_t nregs = rename(e.out, e.trgs);
-    if (nregs <= MAX_REGS || pass == 1) {
-      emit(book, e.out, nregs, d);
-      return nregs;
+    if (pass == 0 || nregs < best_regs) {
+      best = std::move(e.out);
+      best_regs = nregs;
     }
+    if (best_regs <= LOCAL_REGS) break;
   }
-  return 0;
+  emit(book, best, best_regs, d);
+  return best_regs;
 }
 
 void Book::load(const AstBook& b) {

@@ -59,7 +59,12 @@ struct DevDef {  // 32 bytes
 static_assert(sizeof(DevInstr) == 16, "DevInstr layout");
 static_assert(sizeof(DevDef) == 32, "DevDef layout");
 
-constexpr uint32_t MAX_REGS = 48;  // device register file per call
+// A Def call's registers: up to LOCAL_REGS in the calling thread's local
+// memory; more (up to MAX_REGS, the reach of a DevInstr's one-byte register
+// indices) in a per-lane register file in device memory, which a run
+// allocates only when its Book has such a Def.
+constexpr uint32_t LOCAL_REGS = 48;
+constexpr uint32_t MAX_REGS = 256;
 
 struct LabSet {  // runtime/src/def.rs:7-62
   uint16_t min_safe = 0;
@@ -123,6 +128,11 @@ struct Book {
   // (Host::encode_net, host/src/encode.rs:116-120).  Returns its def index.
   uint32_t add_expr(const AstNet& net);
   uint32_t def_count() const { return uint32_t(names.size()); }
+  uint32_t max_nregs() const {
+    uint32_t m = 0;
+    for (const DevDef& d : defs) m = d.nregs > m ? d.nregs : m;
+    return m;
+  }
 };
 
 // Reads the net rooted at heap word `root` out of a heap image

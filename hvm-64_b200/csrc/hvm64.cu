@@ -357,6 +357,7 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
     W.ring_cap = 0;
     const ull gw = ull(blockIdx.x) * WARPS + (threadIdx.x >> 5);
     W.sp = g_P.spill ? g_P.spill + 2ull * g_P.spill_cap * gw : nullptr;
+    W.bigregs = g_P.bigregs ? g_P.bigregs + ull(32 * MAX_REGS) * gw : nullptr;
     W.sp_cap = g_P.spill ? g_P.spill_cap : 0u;
     W.sp_n = 0;
     W.st_steps = W.st_lanes = W.st_busy = W.st_idle = W.st_lane_sum = W.st_lane_max = 0;
@@ -751,6 +752,8 @@ __global__ void __launch_bounds__(THREADS) boot_kernel(unsigned first, unsigned 
     W.pool_cap = 0;
     W.sp = nullptr;
     W.sp_n = W.sp_cap = 0;
+    const ull gw = ull(blockIdx.x) * WARPS + (threadIdx.x >> 5);
+    W.bigregs = g_P.bigregs ? g_P.bigregs + ull(32 * MAX_REGS) * gw : nullptr;
     lane_init(&W, 0);
   }
   const unsigned stride = gridDim.x * WARPS;
@@ -1016,17 +1019,23 @@ struct Runner {
     p.spill = spill.p;
     p.spill_cap = spill_cap;
     p.ovf_flush = dev::OVF_FLUSH;
+    p.bigregs = bigregs.p;
     return p;
   }
 
   // The reducer grid for a tuning, and the warps' overflow stacks sized to it.
   DevBuf<dev::ull> spill;
   unsigned spill_cap = 0, grid = 0;
+  DevBuf<dev::ull> bigregs;
   void prepare_grid(const hvm64_tuning& t) {
     grid = unsigned(sms * reducer_blocks_per_sm(t));
     uint64_t warps = uint64_t(grid) * dev::WARPS;
     spill_cap = spill_cap_for(heap_bytes, warps);
     spill.alloc(2 * size_t(spill_cap) * warps);
+    if (book.max_nregs() > LOCAL_REGS) {  // for the reducer's warps and the boot kernel's
+      uint64_t w = std::max<uint64_t>(grid, uint64_t(sms) * 8) * dev::WARPS;
+      bigregs.alloc(size_t(w) * 32 * MAX_REGS);
+    }
   }
 
   // Reduce nets [first, first+count) (the rest stay untouched); the grid is
@@ -1425,7 +1434,7 @@ struct Server {
   DevBuf<DevInstr> d_instrs;
   DevBuf<dev::ull> d_labbits;
   DevBuf<dev::ServeReq> req;
-  DevBuf<dev::ull> spill;
+  DevBuf<dev::ull> spill, bigregs;
   dev::ServeDone* done = nullptr;  // mapped host memory
   dev::ull* out = nullptr;         // mapped host memory
   dev::ServeReq* req_stage = nullptr;  // pinned staging for the async copies
@@ -1541,6 +1550,10 @@ struct Server {
     p.spill_cap = spill_cap_for(heap_bytes, warps);
     spill.alloc(2 * size_t(p.spill_cap) * warps);
     p.spill = spill.p;
+    if (book.max_nregs() > LOCAL_REGS) {
+      bigregs.alloc(size_t(warps) * 32 * MAX_REGS);
+      p.bigregs = bigregs.p;
+    }
     turn.take(device, t.timeout_ms ? t.timeout_ms : 120000, true);  // held until shutdown
     upload_params(p, ks);
     CU(cudaStreamSynchronize(ks));  // tables and parameters in place before the reducer starts
@@ -1928,6 +1941,10 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   uint64_t defs_b = book.defs.size() * sizeof(DevDef), ins_b = book.instrs.size() * sizeof(DevInstr);
   uint64_t lab_b = book.labbits.size() * 8;
   uint64_t off_ins = round_up(defs_b), off_lab = off_ins + round_up(ins_b);
+  if (book.max_nregs() > LOCAL_REGS)
+    throw Error(HVM64_ERR_BAD_INPUT, "a definition of this Book needs " + std::to_string(book.max_nregs()) +
+                                         " registers; the no-allocation entry point runs Defs of up to " +
+                                         std::to_string(LOCAL_REGS));
   if (off_lab + lab_b > BOOK_BYTES)
     throw Error(HVM64_ERR_BAD_INPUT, "Book too large for the no-allocation entry point: its device tables need " +
                                          std::to_string(off_lab + lab_b) + " bytes, the limit is " +

@@ -75,8 +75,9 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsig
   // Every other lane has no reuse pool: its reclaimed nodes all go through
   // its free list and, in batches, the shared free stack.
   if (index & 1) W->pool_cap = 0;
-  std::vector<ull> spill(2 * size_t(spill_cap) + 2);
+  std::vector<ull> spill(2 * size_t(spill_cap) + 2), bigregs(32 * MAX_REGS);
   W->sp = spill_cap ? spill.data() : nullptr;
+  W->bigregs = bigregs.data();
   W->sp_cap = spill_cap;
   W->sp_n = 0;
   Ctx c{W.get(), 0, 0};
@@ -210,6 +211,8 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     g_emu = &E;
     {
       auto W = new_warp();
+      std::vector<ull> boot_regs(32 * MAX_REGS);
+      W->bigregs = boot_regs.data();
       W->ring_cap = 0;  // boot redexes go straight to the shared queue
       Ctx c{W.get(), 0, 0};
       ull root = alloc(c);

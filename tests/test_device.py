@@ -302,3 +302,23 @@ def test_concurrent_handles_two_threads():
     assert not errs, errs
     for k in (0, 1):
         assert got[k] == [want[k]] * 4
+
+
+@pytest.mark.gpu
+def test_def_with_many_live_wires():
+    """A Def needing more live wires than a thread's local register file (121
+    in either emission order) runs through the warp's register file in device
+    memory: normal form and counts equal the oracle's."""
+    hvm64, oracle = _hvm(), _oracle()
+    vs = [f"x{i}" for i in range(120)]
+
+    def chain(names):
+        t = "*"
+        for v in reversed(names):
+            t = f"({v} {t})"
+        return t
+    src = f"@wide = ({chain(vs)} {chain(vs[::-1])})\n@main = x & @wide ~ x\n"
+    want, want_rw, _ = oracle.run_book(src)
+    got, rw = hvm64.run_book(src, heap_bytes=1 << 28)
+    assert got == want
+    assert rw == want_rw

@@ -92,3 +92,23 @@ def test_emu_radix_bursts(ring, spill):
     text, rw = emu_run(s, threads=16, ring=ring, spill=spill)
     assert text == want
     assert rw == want_rw
+
+
+def test_emu_def_with_many_live_wires():
+    """A Def whose two halves each hold the same 120 variables needs more
+    than 120 live wires in either emission order: more than a thread's local
+    register file, so its calls use the warp's register file in device
+    memory.  Normal form and counts equal the oracle's."""
+    from oracle import oracle
+    vs = [f"x{i}" for i in range(120)]
+
+    def chain(names):
+        t = "*"
+        for v in reversed(names):
+            t = f"({v} {t})"
+        return t
+    src = f"@wide = ({chain(vs)} {chain(vs[::-1])})\n@main = x & @wide ~ x\n"
+    want, want_rw, _ = oracle.run_book(src)
+    text, rw = emu_run(src, threads=4)
+    assert text == want
+    assert rw == want_rw

@@ -87,6 +87,13 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
     with pytest.raises(hvm64.HvmError) as e:
         hvm64.normal_noalloc(big, "main")
     assert e.value.code == hvm64.ERR_BAD_INPUT and "too large" in str(e.value)
+    # a Def needing more registers than a thread's local register file (the
+    # allocating entry points give it a register file in device memory)
+    wide = hvm64.Book.from_str("@main = (" + "".join(f"(x{i} " for i in range(60)) + "*" + ")" * 60 + " "
+                               + "".join(f"(x{i} " for i in reversed(range(60))) + "*" + ")" * 60 + ")\n")
+    with pytest.raises(hvm64.HvmError) as e:
+        hvm64.normal_noalloc(wide, "main")
+    assert e.value.code == hvm64.ERR_BAD_INPUT and "registers" in str(e.value)
     # a net that outgrows the built-in heap (a generated tree of 2^22 leaves,
     # kept whole: far more than its 3.35 million nodes) stops with OOM, and
     # the next call works
