@@ -1336,10 +1336,13 @@ struct Runner {
     DeviceTurn turn(device, 600000);
     upload_params(params(), 0);
     d_gcount.alloc(n);
-    unsigned blocks = (cnt + 127) / 128;
+    // one thread per net; small blocks spread the (latency-bound) walks over
+    // as many SMs as there are warps of nets
+    constexpr unsigned GB = 32;
+    unsigned blocks = (cnt + GB - 1) / GB;
     gcount.assign(n, ~0u);
     if (cnt) CU(cudaMemcpy(d_gcount.p, gcount.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
-    if (cnt) dev::gather_kernel<<<blocks, 128>>>(first, cnt, d_gcount.p, nullptr, nullptr);
+    if (cnt) dev::gather_kernel<<<blocks, GB>>>(first, cnt, d_gcount.p, nullptr, nullptr);
     CU(cudaGetLastError());
     CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     for (unsigned i = 0; i < n; i++)
@@ -1353,7 +1356,7 @@ struct Runner {
     d_goff.alloc(n);
     CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
     d_gpairs.alloc(2 * tot);
-    if (cnt) dev::gather_kernel<<<blocks, 128>>>(first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
+    if (cnt) dev::gather_kernel<<<blocks, GB>>>(first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
     CU(cudaGetLastError());
     gpairs.resize(2 * tot);
     if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
