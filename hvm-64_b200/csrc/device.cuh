@@ -18,6 +18,7 @@
 // protocol fault can never become a memory fault.
 #pragma once
 #include <stdint.h>
+#include <stddef.h>
 
 #ifndef __CUDACC__
 #include <atomic>
@@ -321,8 +322,10 @@ HVM_INL unsigned redex_class(ull a, ull b) {
 }
 
 // Per-warp shared state of the reducer (one per warp; the CPU emulation
-// harness gives each host thread one too).
-struct WarpSmem {
+// harness gives each host thread one too).  Warps' states lie back to back in
+// shared memory and `icache` is filled with 16-byte stores, so the size is
+// kept a multiple of 16.
+struct alignas(16) WarpSmem {
   ull stk[2 * SCAP];          // redex stack (ring of SCAP pairs)
   ull regs[SMALL_REGS * 32];  // VM registers, [register][lane]
   ull pool[POOL];             // free nodes ready for reuse
@@ -352,6 +355,8 @@ struct WarpSmem {
   int freed_n;
   unsigned pad;
 };
+static_assert(sizeof(WarpSmem) % 16 == 0 && offsetof(WarpSmem, icache) % 16 == 0,
+              "icache of every warp's state must be 16-byte aligned");
 
 // Initial per-lane / per-warp runtime state (lane `ln` of warp state `W`).
 HVM_INL void lane_init(WarpSmem* W, unsigned ln) {
