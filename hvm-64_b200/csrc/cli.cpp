@@ -1,15 +1,22 @@
 // hvm64 -- command line front end of the B200 reducer (the reference's
-// `hvm64 run` / `hvm64 reduce`, src/main.rs:32-204 and src/args.rs), calling
-// only the C ABI in hvm64.h.
+// `hvm64 run` / `hvm64 reduce` / `hvm64 transform`, src/main.rs:32-204 and
+// src/args.rs), calling only the C ABI in hvm64.h.
 //
-//   hvm64 run FILE [ARGS..] [-e ENTRY] [-m MEM] [-s]
-//   hvm64 reduce [FILES..] [-m MEM] [-s] -- EXPRS..
+//   hvm64 run FILE [ARGS..] [-e ENTRY] [-m MEM] [-s] [TRANSFORM OPTS]
+//   hvm64 reduce [FILES..] [-m MEM] [-s] [TRANSFORM OPTS] -- EXPRS..
+//   hvm64 transform [FILES..] [TRANSFORM OPTS]
 //
 // `run` boots ENTRY (default main) applied to each ARG in turn
 // (apply_tree, src/main.rs:195-204); `reduce` normalises each expression
 // against the Book of FILES.  Each normal form goes to stdout; with -s the
 // Rewrites block and TIME / RPS go to stderr as the reference prints them.
 // --print-net prints the net that would be reduced instead of reducing it.
+// `transform` prints the Book after its passes (src/main.rs:71-74).
+// TRANSFORM OPTS (src/args.rs:43-133): -O PASSES (pre-reduce | pre, all, and
+// their no- forms; the Book passes eta-reduce, inline and prune are not part
+// of this build), --pre-reduce-skip NAMES, --pre-reduce-memory MEM,
+// --pre-reduce-rewrites N (default 100M).  `run` never pre-reduces its entry
+// (src/main.rs:58-61).
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -23,8 +30,31 @@ namespace {
 
 void usage() {
   fprintf(stderr,
-          "usage: hvm64 run FILE [ARGS..] [-e ENTRY] [-m MEM] [-s]\n"
-          "       hvm64 reduce [FILES..] [-m MEM] [-s] -- EXPRS..\n");
+          "usage: hvm64 run FILE [ARGS..] [-e ENTRY] [-m MEM] [-s] [-O PASSES]\n"
+          "       hvm64 reduce [FILES..] [-m MEM] [-s] [-O PASSES] -- EXPRS..\n"
+          "       hvm64 transform [FILES..] [-O PASSES] [--pre-reduce-skip NAMES]\n"
+          "                       [--pre-reduce-memory MEM] [--pre-reduce-rewrites N]\n");
+}
+
+// -O values (src/args.rs:128-133 and the `all` switch): the pass flags in
+// the order given, the last word winning.  Returns false on an unknown name.
+struct Passes {
+  bool pre_reduce = false, eta = false, inline_ = false, prune = false;
+};
+bool apply_pass(const std::string& word, Passes* p) {
+  bool on = true;
+  std::string w = word;
+  if (w.rfind("no-", 0) == 0) {
+    on = false;
+    w = w.substr(3);
+  }
+  if (w == "all") *p = Passes{on, on, on, on};
+  else if (w == "pre-reduce" || w == "pre") p->pre_reduce = on;
+  else if (w == "eta-reduce" || w == "eta") p->eta = on;
+  else if (w == "inline") p->inline_ = on;
+  else if (w == "prune") p->prune = on;
+  else return false;
+  return true;
 }
 
 // util/src/parse_abbrev_number.rs: a number with an optional K/M/G/T suffix.
@@ -112,20 +142,45 @@ int main(int argc, char** argv) {
     return 2;
   }
   std::string mode = argv[1];
-  if (mode != "run" && mode != "reduce") {
+  if (mode != "run" && mode != "reduce" && mode != "transform") {
     usage();
     return 2;
   }
   std::vector<std::string> files, args, exprs;
-  std::string entry = "main";
-  unsigned long long mem = 0;
+  std::string entry = "main", skip;
+  unsigned long long mem = 0, pre_mem = 0, pre_rwts = 100ull << 20;
   bool stats = false, after_dd = false, print_only = false;
+  Passes passes;
   for (int k = 2; k < argc; k++) {
     std::string a = argv[k];
     if (after_dd) {
       exprs.push_back(a);
     } else if (a == "--") {
       after_dd = true;
+    } else if (a.rfind("-O", 0) == 0) {
+      std::string v = a.size() > 2 ? a.substr(2) : (k + 1 < argc ? std::string(argv[++k]) : std::string());
+      size_t s0 = 0;
+      while (s0 <= v.size()) {  // value_delimiter ' '
+        size_t e = v.find(' ', s0);
+        if (e == std::string::npos) e = v.size();
+        if (e > s0 && !apply_pass(v.substr(s0, e - s0), &passes)) {
+          fprintf(stderr, "error: unknown transform pass %s\n", v.substr(s0, e - s0).c_str());
+          return 2;
+        }
+        s0 = e + 1;
+      }
+    } else if (a == "--pre-reduce-skip" && k + 1 < argc) {
+      skip += std::string(argv[++k]) + " ";
+    } else if (a == "--pre-reduce-memory" && k + 1 < argc) {
+      if (!parse_mem(argv[++k], &pre_mem)) {
+        fprintf(stderr, "error: bad memory size %s\n", argv[k]);
+        return 2;
+      }
+    } else if (a == "--pre-reduce-rewrites" && k + 1 < argc) {
+      if (!parse_mem(argv[++k], &pre_rwts)) {
+        fprintf(stderr, "error: bad rewrite count %s\n", argv[k]);
+        return 2;
+      }
     } else if (a == "-s" || a == "--stats") {
       stats = true;
     } else if (a == "--print-net") {
@@ -158,6 +213,37 @@ int main(int argc, char** argv) {
       return 1;
     }
     text += "\n";
+  }
+  if (passes.eta || passes.inline_ || passes.prune) {
+    fprintf(stderr, "error: only the pre-reduce transform is part of this build\n");
+    return 2;
+  }
+  if (passes.pre_reduce) {  // Book::transform (transform/src/transform.rs:35-77)
+    if (mode == "run") skip += entry;
+    size_t len = 0, nlen = 0;
+    std::string out(4 * text.size() + 4096, '\0'), nn(4096, '\0');
+    for (int pass = 0; pass < 2; pass++) {
+      if (hvm64_pre_reduce(text.data(), text.size(), skip.c_str(), pre_rwts, pre_mem, nullptr, nullptr, &out[0],
+                           out.size(), &len, &nn[0], nn.size(), &nlen))
+        return fail("pre-reducing");
+      if (len < out.size() && nlen < nn.size()) break;
+      out.assign(len + 1, '\0');  // the Book outgrew the buffer: size it and run again
+      nn.assign(nlen + 1, '\0');
+    }
+    out.resize(len);
+    text = out + "\n";
+  }
+  if (mode == "transform") {  // src/main.rs:71-74: println!("{}", book)
+    if (!passes.pre_reduce) {
+      size_t len = 0;
+      if (hvm64_book_format(text.data(), text.size(), nullptr, 0, &len)) return fail("parsing the book");
+      std::string out(len + 1, '\0');
+      hvm64_book_format(text.data(), text.size(), &out[0], out.size(), &len);
+      out.resize(len);
+      text = out + "\n";
+    }
+    printf("%s", text.c_str());
+    return 0;
   }
   std::vector<std::string> nets;
   if (mode == "run") nets.push_back(run_net(entry, args));

@@ -98,7 +98,9 @@ struct Ctrl {
   ull pad8[14];
   ull free_top;       // shared stack of free-node batches: batch head address | push count << 44
   ull reuse_mark;     // bump position from which free nodes are shared between warps
-  ull pad9[14];
+  ull captured;       // pre-reduce: redexes recorded by inert Defs (see capture)
+  ull rw_done;        // interactions folded so far, when the run has an interaction limit
+  ull pad9[12];
 };
 
 constexpr int NCOUNT = 8;  // rw[5] then comm22, dref_nodes, dref_links
@@ -157,6 +159,12 @@ struct Params {
   // register files of Def calls needing more than LOCAL_REGS registers:
   // warp g owns bigregs[32 * MAX_REGS * g ...], [register][lane]; null: none
   ull* bigregs;
+  // pre-reduce (all zero otherwise): boot without the expansion agent
+  // (Net::reduce after Net::boot, transform/src/pre_reduce.rs:145-147); the
+  // buffer for redexes inert Defs capture; an interaction limit
+  unsigned no_expand, capture_cap;
+  ull* capture;
+  ull rw_limit;
   // serving (all zero for a batch run)
   unsigned serve;
   const ServeReq* req;         // device ring of req_cap requests
@@ -1016,6 +1024,14 @@ HVM_COLD void do_switch(const Ctx& c, ull trg, ull& o1, ull& o2) {
   o2 = pvar(m ^ 8);
 }
 // Runs a Def's instruction list over a register file (base + i * stride).
+// An inert Def's call (transform/src/pre_reduce.rs:96-101): the redex is
+// recorded for the host, which puts it back into the net's redexes.
+HVM_COLD void capture(const Ctx& c, ull port, ull trg) {
+  ull k = atom_add(&g_P.ctrl->captured, 1ull);
+  if (k >= g_P.capture_cap) return run_fail(c.net, HVM64_ERR_OUTPUT, k);
+  g_P.capture[2 * k] = port;
+  g_P.capture[2 * k + 1] = trg;
+}
 HVM_COLD void exec(const Ctx& c, const DevDef& d, ull t0, ull* R, unsigned stride, const DevInstr* ins) {
   R[0] = t0;
   for (unsigned k = 0; k < d.ins_len; k++) {
@@ -1037,6 +1053,7 @@ HVM_COLD void exec(const Ctx& c, const DevDef& d, ull t0, ull* R, unsigned strid
         R[I.d * stride] = a ^ 8;
         break;
       }
+      case I_CAPTURE: capture(c, I.port, *ra); break;
     }
   }
 }

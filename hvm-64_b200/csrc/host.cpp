@@ -10,6 +10,7 @@
 #include <cstring>
 #include <exception>
 #include <optional>
+#include <set>
 #include <unordered_map>
 
 #include "hvm64.h"
@@ -392,6 +393,12 @@ bool LabSet::has(uint16_t lab) const {
   size_t w = lab >> 6;
   return w < bits.size() && ((bits[w] >> (lab & 63)) & 1);
 }
+LabSet LabSet::all() {
+  LabSet s;
+  s.min_safe = 0xFFFF;
+  s.bits.assign(1024, ~uint64_t(0));
+  return s;
+}
 void LabSet::unite(const LabSet& o) {
   min_safe = std::max(min_safe, o.min_safe);
   if (o.bits.size() > bits.size()) bits.resize(o.bits.size(), 0);
@@ -405,6 +412,7 @@ struct Labeler {
   const AstBook& book;
   struct St { bool done; LabSet labs; size_t head; };
   std::map<std::string, St> memo;
+  std::set<std::string>* missing = nullptr;  // collects absent references (null: they are errors)
 
   size_t def(const std::string& key, std::optional<size_t> depth, LabSet* out) {
     auto it = memo.find(key);
@@ -444,9 +452,13 @@ struct Labeler {
   size_t tree(const Tree* t, std::optional<size_t> depth, LabSet* out) {
     if (t->kind == K_CTR && out) out->add(t->lab);
     if (t->kind == K_REF) {
-      if (!book.nets.count(t->name))
+      if (book.nets.count(t->name))
+        return def(t->name, depth ? std::optional<size_t>(*depth + 1) : std::nullopt, out);
+      if (!missing)
         throw Error(HVM64_ERR_BAD_INPUT, "Found reference \"" + t->name + "\", which is not in the book!");
-      return def(t->name, depth ? std::optional<size_t>(*depth + 1) : std::nullopt, out);
+      missing->insert(t->name);
+      if (out) out->unite(LabSet::all());
+      return SIZE_MAX;
     }
     size_t h = SIZE_MAX;
     if (t->p1) h = std::min(h, tree(t->p1, depth, out));
@@ -675,21 +687,44 @@ static uint32_t encode_net(Book& book, const AstNet& net, DevDef& d) {
   return best_regs;
 }
 
-void Book::load(const AstBook& b) {
+void Book::load(const AstBook& b, bool inert_missing) {
   keep.push_back(b.arena);
   // Phase 1: ids and label sets (host.rs:54-65); phase 2: instructions.
   for (auto& [name, _] : b.nets) {
     ids[name] = uint32_t(names.size());
     names.push_back(name);
   }
-  Labeler L{b, {}};
+  std::set<std::string> missing;
+  Labeler L{b, {}, inert_missing ? &missing : nullptr};
   for (auto& [name, _] : b.nets) L.def(name, 0, nullptr);
+  for (const std::string& name : missing) {
+    ids[name] = uint32_t(names.size());
+    names.push_back(name);
+  }
   labs.resize(names.size());
   for (auto& [name, st] : L.memo) {
     if (!st.done) throw Error(HVM64_ERR_BAD_INPUT, "label analysis did not converge");
     labs[ids[name]] = st.labs;
   }
   defs.resize(names.size());
+  for (const std::string& name : missing) {  // pre_reduce.rs:89-102 (InertDef)
+    uint32_t id = ids[name];
+    labs[id] = LabSet::all();
+    DevDef d{};
+    d.ins_off = uint32_t(instrs.size());
+    d.ins_len = 1;
+    d.nregs = 1;
+    d.flags = DEF_INERT;
+    d.min_safe = labs[id].min_safe;
+    d.lab_off = uint32_t(labbits.size());
+    d.lab_len = uint32_t(labs[id].bits.size());
+    labbits.insert(labbits.end(), labs[id].bits.begin(), labs[id].bits.end());
+    DevInstr x{};
+    x.k = I_CAPTURE;
+    x.port = ref_port(id, d.min_safe);
+    instrs.push_back(x);
+    defs[id] = d;
+  }
   for (auto& [name, net] : b.nets) {
     uint32_t id = ids[name];
     DevDef d{};
@@ -702,13 +737,21 @@ void Book::load(const AstBook& b) {
   }
 }
 
+void Book::replace_def(uint32_t id, const AstNet& net) {
+  if (id >= defs.size()) throw Error(HVM64_ERR_BAD_INPUT, "no such definition");
+  DevDef d = defs[id];
+  encode_net(*this, net, d);
+  d.flags = uint16_t(d.flags & ~DEF_INERT);
+  defs[id] = d;
+}
+
 uint32_t Book::add_expr(const AstNet& net) {
   DevDef d{};
   encode_net(*this, net, d);
   d.min_safe = 0;
   d.lab_off = 0;
   d.lab_len = 0;
-  d.flags = 1;  // expression program: no DREF is counted for it
+  d.flags = DEF_EXPR;  // expression program: no DREF is counted for it
   defs.push_back(d);
   return uint32_t(defs.size() - 1);
 }
@@ -821,6 +864,92 @@ struct Reader {
 std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root) {
   Reader r{book, heap, heap_words, {}, 0, {}};
   r.wire(root);
+  return r.o;
+}
+
+// ===========================================================================
+// Pre-reduce driver (transform/src/pre_reduce.rs:38-74,136-164)
+// ===========================================================================
+namespace {
+struct PreReduceDfs {
+  const AstBook& ast;
+  Book& book;
+  const std::set<std::string>& skip;
+  uint64_t max_rwts;
+  const std::function<PreReduceRun(uint32_t)>& run_one;
+  std::map<std::string, int> seen;  // 0: on the path ("Cycled"), 1: done
+  std::map<std::string, std::string> reduced;
+  PreReduceOut out;
+
+  void visit_tree(const Tree* t) {  // pre_reduce.rs:122-129
+    if (t->kind == K_REF) visit(t->name);
+    if (t->p1) visit_tree(t->p1);
+    if (t->p2) visit_tree(t->p2);
+  }
+  void visit(const std::string& name) {  // pre_reduce.rs:137-164
+    auto src = ast.nets.find(name);
+    if (seen.count(name) || skip.count(name) || src == ast.nets.end()) return;
+    seen[name] = 0;
+    visit_tree(src->second.root);
+    for (auto& rd : src->second.redexes) {
+      visit_tree(rd.first);
+      visit_tree(rd.second);
+    }
+    const uint32_t id = book.ids.at(name);
+    PreReduceRun r = run_one(id);
+    out.runs++;
+    seen[name] = 1;
+    if (r.status && r.status != HVM64_ERR_LIMIT)
+      throw Error(r.status, "pre-reducing @" + name + ": " + r.error);
+    // Net::reduce(limit) reports normal form when fewer than `limit` redexes
+    // were popped (net.rs:41-52).
+    if (r.status == HVM64_ERR_LIMIT || r.pops >= max_rwts) {
+      // The reference keeps the net as it stood after max_rwts pops; a device
+      // run does not stop at an exact pop, so the Def keeps its original net
+      // (and adds no Rewrites).  Either way it is reported as not normal.
+      out.not_normal.push_back(name);
+      return;
+    }
+    for (int k = 0; k < 5; k++) out.rw[k] += r.rw[k];
+    Arena arena;
+    AstNet net = parse_net(r.text, arena);
+    book.replace_def(id, net);
+    reduced[name] = std::move(r.text);
+  }
+};
+}  // namespace
+
+std::string print_book(const AstBook& b) {
+  std::string o;
+  for (auto& [name, net] : b.nets) {
+    if (!o.empty()) o += "\n\n";
+    o += "@" + name + " = " + print_net(net);
+  }
+  return o;
+}
+
+PreReduceOut pre_reduce(const AstBook& ast, Book& book, const std::set<std::string>& skip, uint64_t max_rwts,
+                        const std::function<PreReduceRun(uint32_t)>& run_one) {
+  PreReduceDfs d{ast, book, skip, max_rwts, run_one, {}, {}, {}};
+  for (auto& [name, _] : ast.nets) d.visit(name);
+  for (auto& [name, net] : ast.nets) {  // pre_reduce.rs:60-67, then ast.rs:221-232
+    if (!d.out.text.empty()) d.out.text += "\n\n";
+    auto it = d.reduced.find(name);
+    d.out.text += "@" + name + " = " + (it != d.reduced.end() ? it->second : print_net(net));
+  }
+  return std::move(d.out);
+}
+
+std::string readback_net(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root,
+                         const uint64_t* redexes, size_t nredexes) {
+  Reader r{book, heap, heap_words, {}, 0, {}};
+  r.wire(root);
+  for (size_t i = 0; i < nredexes; i++) {  // host/src/readback.rs:28-30
+    r.o += "\n  & ";
+    r.port(redexes[2 * i], 0);
+    r.o += " ~ ";
+    r.port(redexes[2 * i + 1], 0);
+  }
   return r.o;
 }
 

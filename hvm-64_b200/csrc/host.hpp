@@ -9,6 +9,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -37,7 +38,10 @@ inline uint64_t ref_port(uint32_t def_id, uint16_t min_safe) { return port_new(T
 // runtime/src/instruction.rs:34-72) over a small register file; TrgIds are
 // renamed to registers by linear scan (each TrgId is written once and read
 // once), register 0 being the Def's argument port.
-enum InstrKind : uint8_t { I_CONST, I_LINK, I_LINKCONST, I_CTR, I_OP, I_OPNUM, I_SWITCH, I_WIRES };
+// I_CAPTURE is the whole body of an inert Def (a reference a Book being
+// pre-reduced lacks, transform/src/pre_reduce.rs:89-102): the call's redex
+// (`port`, register a) is recorded for the host instead of expanded.
+enum InstrKind : uint8_t { I_CONST, I_LINK, I_LINKCONST, I_CTR, I_OP, I_OPNUM, I_SWITCH, I_WIRES, I_CAPTURE };
 
 struct DevInstr {  // 16 bytes
   uint8_t k;
@@ -52,10 +56,12 @@ struct DevDef {  // 32 bytes
   uint32_t nregs;
   uint32_t lab_off, lab_len;  // label bitset words in the shared table
   uint16_t min_safe;
-  uint16_t flags;
+  uint16_t flags;  // DEF_EXPR | DEF_INERT
   uint32_t nodes;  // upper bound on nodes one call allocates
   uint32_t redexes;
 };
+constexpr uint16_t DEF_EXPR = 1;   // an expression program: booting it counts no DREF
+constexpr uint16_t DEF_INERT = 2;  // an inert Def (pre-reduce): its body is one I_CAPTURE
 static_assert(sizeof(DevInstr) == 16, "DevInstr layout");
 static_assert(sizeof(DevDef) == 32, "DevDef layout");
 
@@ -72,6 +78,7 @@ struct LabSet {  // runtime/src/def.rs:7-62
   void add(uint16_t lab);
   bool has(uint16_t lab) const;
   void unite(const LabSet& o);
+  static LabSet all();  // LabSet::ALL (runtime/src/def.rs:17)
 };
 
 // ---- AST (ast/src/ast.rs) -------------------------------------------------
@@ -109,6 +116,7 @@ AstNet parse_net(const std::string& text, Arena& arena);
 Tree* parse_tree(const std::string& text, Arena& arena);
 std::string print_tree(const Tree* t);
 std::string print_net(const AstNet& n);
+std::string print_book(const AstBook& b);  // ast.rs:221-232
 std::string num_to_string(uint32_t n);
 void apply_tree(AstNet& net, Tree* arg, Arena& arena);
 
@@ -122,8 +130,14 @@ struct Book {
   std::vector<uint64_t> labbits;
   std::vector<std::shared_ptr<Arena>> keep;
 
-  // Loads a Book (Host::insert_book, host/src/host.rs:34-73).
-  void load(const AstBook& b);
+  // Loads a Book (Host::insert_book, host/src/host.rs:34-73).  With
+  // `inert_missing`, a reference the Book lacks becomes an inert Def with
+  // LabSet::ALL (insert_book_with_default as transform/src/pre_reduce.rs:41
+  // calls it) instead of an error.
+  void load(const AstBook& b, bool inert_missing = false);
+  // Replaces Def `id`'s instructions by the encoding of `net`, keeping its
+  // label set (pre_reduce.rs:155-157: encode_def into the existing Def).
+  void replace_def(uint32_t id, const AstNet& net);
   // Encodes an expression net as a program run against the root
   // (Host::encode_net, host/src/encode.rs:116-120).  Returns its def index.
   uint32_t add_expr(const AstNet& net);
@@ -139,6 +153,10 @@ struct Book {
 // (Host::readback, host/src/readback.rs:23-87).  Redirect chains (Red ports
 // left by concurrent linking) are followed to the live endpoint.
 std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root);
+// The same followed by redexes (port pairs, ast.rs:234-244 layout), all
+// sharing one variable naming: Host::readback of a net with redexes.
+std::string readback_net(const Book& book, const uint64_t* heap, uint64_t heap_words, uint64_t root,
+                         const uint64_t* redexes, size_t nredexes);
 // Many nets' normal forms from gathered pairs at once, on `threads` host
 // threads: net i's pairs start at pair offsets[i] and number counts[i]
 // (~0u: not gathered, left empty).  A net that fails keeps its message.
@@ -152,6 +170,32 @@ std::vector<ReadbackOut> readback_pairs_many(const Book& book, const uint64_t* p
 // The same from the (address, word) pairs a serving reducer gathered.
 std::string readback_pairs(const Book& book, const uint64_t* pairs, size_t npairs, uint64_t heap_words,
                            uint64_t root);
+
+// Book::pre_reduce (transform/src/pre_reduce.rs:38-74,136-164).  Each Def
+// of `ast` not in `skip` is visited in byte order of names and first visits
+// the Defs its original net references, depth first (a Def met again while
+// still on that path is used as it is: the reference's "Cycled" state).  Then
+// `run_one(id)` boots Def `id` of `book` alone, without the expansion agent,
+// and reduces it; the net it reads back replaces the Def's instructions in
+// `book` at once (so later Defs call the reduced version) and the Def's text
+// in the result.  Label sets stay those of the original Book, as in the
+// reference's Host.  `book` must have been loaded from `ast` with
+// inert_missing.
+struct PreReduceRun {
+  int status = 0;         // HVM64_OK, HVM64_ERR_LIMIT (stopped early), or an error
+  uint64_t pops = 0;      // redexes the reduction popped (Net::reduce's count)
+  uint64_t rw[5] = {0};   // anni, comm, eras, dref, oper
+  std::string text;       // the net read back (root, then its redexes)
+  std::string error;
+};
+struct PreReduceOut {
+  std::string text;       // the pre-reduced Book (ast.rs:221-232 Display)
+  uint64_t rw[5] = {0};
+  std::vector<std::string> not_normal;
+  uint32_t runs = 0;
+};
+PreReduceOut pre_reduce(const AstBook& ast, Book& book, const std::set<std::string>& skip, uint64_t max_rwts,
+                        const std::function<PreReduceRun(uint32_t)>& run_one);
 
 // Runs f on a thread with a large stack (deep trees recurse; the reference
 // grows its stack with `stacker`, util/src/maybe_grow.rs).

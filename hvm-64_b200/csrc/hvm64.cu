@@ -24,6 +24,7 @@
 #include <condition_variable>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -169,7 +170,25 @@ __device__ __forceinline__ void fold_counts(WarpSmem& W) {
   __syncwarp();
 }
 
-__device__ __noinline__ void fold_counts_cold(WarpSmem& W) { fold_counts(W); }
+// The same, out of line; a run with an interaction limit also adds what was
+// folded to the run's total and stops the run once the total passes the
+// limit (Net::reduce(limit), runtime/src/net.rs:41-52; checked every fold, so
+// a run may overshoot by what its warps do between folds).
+__device__ __noinline__ void fold_counts_cold(WarpSmem& W, int cur) {
+  const unsigned lane = threadIdx.x & 31;
+  __syncwarp();
+  ull done = 0;
+#pragma unroll
+  for (int k = 0; k < NCOUNT; k++) {
+    unsigned v = __reduce_add_sync(0xffffffffu, W.cnt[k * 32 + lane]);
+    W.cnt[k * 32 + lane] = 0;
+    if (lane == 0 && v) W.rw[k] += v;
+    if (k <= RW_OPER) done += v;
+  }
+  if (lane == 0 && g_P.rw_limit && done && atomicAdd(&g_P.ctrl->rw_done, done) + done > g_P.rw_limit)
+    run_fail(unsigned(cur), HVM64_ERR_LIMIT, g_P.rw_limit);
+  __syncwarp();
+}
 
 // Flush the warp's counters into its net (one atomic per counter).
 __device__ void flush_counters(WarpSmem& W, int cur) {
@@ -669,7 +688,7 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
     // The lanes' counters fold into the warp's when it lets its net go, and
     // out of line every 4096 steps (which bounds a lane's 32-bit counts);
     // folding every step measured 4 % slower.
-    if ((step & 4095) == 0) fold_counts_cold(W);
+    if ((step & 4095) == 0) fold_counts_cold(W, cur);
     else __syncwarp();
     // Nodes reclaimed in this step become allocatable after a fence.
     mem_fence();
@@ -771,8 +790,10 @@ __global__ void __launch_bounds__(THREADS) boot_kernel(unsigned first, unsigned 
       // Small Defs use register slots 0, 32, 64, ... of W.regs (lane 0's column).
       run_def(c, prog, pvar(root));
       settle(c);
-      root = expand(c, root);
-      settle(c);
+      if (!g_P.no_expand) {
+        root = expand(c, root);
+        settle(c);
+      }
       ns.root = root;
     }
     __syncwarp();
@@ -855,6 +876,7 @@ const char* status_name(int s) {
     case HVM64_ERR_QUEUE: return "device redex queue overflow";
     case HVM64_ERR_BAD_ADDR: return "heap address outside the arena";
     case HVM64_ERR_OUTPUT: return "normal form larger than the request's output buffer";
+    case HVM64_ERR_LIMIT: return "interaction limit reached";
   }
   return "unknown error";
 }
@@ -1020,8 +1042,19 @@ struct Runner {
     p.spill_cap = spill_cap;
     p.ovf_flush = dev::OVF_FLUSH;
     p.bigregs = bigregs.p;
+    p.no_expand = no_expand ? 1u : 0u;
+    p.rw_limit = rw_limit;
+    p.capture = capture.p;
+    p.capture_cap = capture.p ? unsigned(capture.n / 2) : 0u;
     return p;
   }
+
+  // Pre-reduce runs (see PreReducer): boot without the expansion agent,
+  // stop past an interaction limit (0: none), and a buffer for the redexes
+  // inert Defs capture.
+  bool no_expand = false;
+  uint64_t rw_limit = 0;
+  DevBuf<dev::ull> capture;
 
   // The reducer grid for a tuning, and the warps' overflow stacks sized to it.
   DevBuf<dev::ull> spill;
@@ -1397,11 +1430,69 @@ struct Runner {
     with_big_stack([&] { out = hvm::readback(book, image.data(), image.size(), host_nets[i].root); });
     return out;
   }
+
+  // Net i of the last run (a pre-reduce run) with the redexes inert Defs
+  // captured: those with an eraser first, each group in capture order.
+  std::string readback_captured(unsigned i) {
+    uint64_t n = std::min<uint64_t>(host_ctrl.captured, capture.n / 2);
+    std::vector<uint64_t> got(2 * n), pairs;
+    if (n) CU(cudaMemcpy(got.data(), capture.p, 16 * n, cudaMemcpyDeviceToHost));
+    d2h += 16 * n;
+    pairs.reserve(got.size());
+    for (int pass = 0; pass < 2; pass++)
+      for (uint64_t k = 0; k < n; k++)
+        if ((got[2 * k + 1] == PORT_ERA) == (pass == 0)) {
+          pairs.push_back(got[2 * k]);
+          pairs.push_back(got[2 * k + 1]);
+        }
+    if (!n) return readback(i);
+    uint64_t used = 0;
+    CU(cudaMemcpy(&used, &ctrl.p->bump, 8, cudaMemcpyDeviceToHost));
+    used = std::min<uint64_t>(used, heap_bytes / 16);
+    image.resize(used * 2);
+    CU(cudaMemcpy(image.data(), heap.p, used * 16, cudaMemcpyDeviceToHost));
+    d2h += used * 16 + 8;
+    image_valid = true;
+    std::string out;
+    with_big_stack([&] {
+      out = hvm::readback_net(book, image.data(), image.size(), host_nets[i].root, pairs.data(), pairs.size() / 2);
+    });
+    return out;
+  }
 };
 
 namespace dev {
 __global__ void set_deadline_kernel(Ctrl* c, ull timeout_ns) { c->deadline = globaltimer() + timeout_ns; }
 }  // namespace dev
+
+// ===========================================================================
+// Pre-reduce (transform/src/pre_reduce.rs:38-74,136-164) on the device
+// ===========================================================================
+// One launch per Def, all on one reused heap (the reference's shared `area`):
+// the Def is booted without the expansion agent and reduced by the
+// persistent reducer.  The redexes inert Defs captured go back into the net
+// after those the reduction left, ones with an eraser first (linker.rs:70-85
+// puts them in the fast queue, which Host::readback lists first).  The host
+// driver (hvm::pre_reduce) orders the Defs and replaces them.
+PreReduceRun pre_reduce_one(Runner& r, uint32_t id, const hvm64_tuning& tuning, double& device_ms) {
+  PreReduceRun out;
+  r.progs.assign(1, id);
+  r.uploaded_defs = 0;  // the instruction table changed since the last launch
+  double ms = 0;
+  r.run(HVM64_BATCH_PERSISTENT, &tuning, &ms);
+  device_ms += ms;
+  const dev::NetState& ns = r.host_nets[0];
+  out.status = ns.status;
+  out.pops = r.stat_lanes;
+  out.rw[0] = ns.rw[dev::RW_ANNI];
+  out.rw[1] = ns.rw[dev::RW_COMM];
+  out.rw[2] = ns.rw[dev::RW_ERAS];
+  out.rw[3] = ns.rw[dev::RW_DREF];
+  out.rw[4] = ns.rw[dev::RW_OPER];
+  if (ns.status) out.error = r.error_message(ns.status);
+  else out.text = r.readback_captured(0);
+  return out;
+}
 
 void Runner::set_deadline(cudaStream_t st, uint64_t timeout_ms) {
   dev::set_deadline_kernel<<<1, 1, 0, st>>>(ctrl.p, uint64_t(timeout_ms) * 1000000ull);
@@ -1871,6 +1962,64 @@ int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
   if (!n || !out) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
   n->r.stats(out);
   return HVM64_OK;
+}
+
+int hvm64_book_format(const char* text, size_t len, char* buf, size_t cap, size_t* out_len) {
+  if (!text) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] {
+    std::string src(text, len), out;
+    hvm::with_big_stack([&] { out = hvm::print_book(hvm::parse_book(src)); });
+    copy_out(out, buf, cap, out_len);
+  });
+}
+
+int hvm64_pre_reduce(const char* text, size_t len, const char* skip, uint64_t max_rwts, uint64_t heap_bytes,
+                     const hvm64_tuning* tuning, hvm64_rewrites* out, char* buf, size_t cap, size_t* out_len,
+                     char* not_normal, size_t nn_cap, size_t* nn_len) {
+  if (!text) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] {
+    hvm::AstBook ast;
+    hvm::Runner r;
+    std::string src(text, len);
+    hvm::with_big_stack([&] {
+      ast = hvm::parse_book(src);
+      r.book.load(ast, true);
+    });
+    // names separated by spaces or newlines (src/args.rs:51: value_delimiter ' ')
+    std::set<std::string> sk;
+    std::string names = skip ? skip : "";
+    size_t s0 = 0;
+    while (s0 <= names.size()) {
+      size_t e = names.find_first_of(" \n", s0);
+      if (e == std::string::npos) e = names.size();
+      if (e > s0) sk.insert(names.substr(s0, e - s0));
+      s0 = e + 1;
+    }
+    hvm64_tuning t{};
+    if (tuning) t = *tuning;
+    r.setup(heap_bytes);
+    r.no_expand = true;
+    if (max_rwts != ~uint64_t(0)) {
+      // A bound on device work only (what counts is the pops, checked after
+      // the run): a popped redex makes at most one plus a Def's instruction
+      // count of interactions.
+      uint64_t per = 1;
+      for (const hvm::DevDef& d : r.book.defs) per = std::max<uint64_t>(per, uint64_t(d.ins_len) + 1);
+      r.rw_limit = max_rwts > ~uint64_t(0) / per ? 0 : std::max<uint64_t>(max_rwts * per, 1);
+    }
+    r.capture.alloc(2 * (size_t(1) << 16));
+    double ms = 0;
+    hvm::PreReduceOut res;
+    hvm::with_big_stack([&] {
+      res = hvm::pre_reduce(ast, r.book, sk, max_rwts,
+                            [&](uint32_t id) { return hvm::pre_reduce_one(r, id, t, ms); });
+    });
+    if (out) *out = hvm64_rewrites{res.rw[0], res.rw[1], res.rw[2], res.rw[3], res.rw[4]};
+    copy_out(res.text, buf, cap, out_len);
+    std::string nn;
+    for (const std::string& n : res.not_normal) nn += n + "\n";
+    copy_out(nn, not_normal, nn_cap, nn_len);
+  });
 }
 
 }  // extern "C"

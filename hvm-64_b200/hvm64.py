@@ -17,7 +17,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HVM64_LIB") or os.path.join(HERE, "build", "libhvm64.so")
 
-OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR, ERR_OUTPUT = range(10)
+OK, ERR_OOM, ERR_BAD_PAIR, ERR_DIV0, ERR_TIMEOUT, ERR_BAD_INPUT, ERR_CUDA, ERR_QUEUE, ERR_BAD_ADDR, ERR_OUTPUT, \
+    ERR_LIMIT = range(11)
 PERSISTENT, PLAIN = 0, 1
 TUNE_GRAPH = 1  # Tuning.flags: persistent runs replay one captured CUDA graph
 
@@ -29,7 +30,7 @@ EXPORTS = (
     "hvm64_batch_free", "hvm64_batch_stats", "hvm64_net_stats", "hvm64_net_normal_noalloc",
     "hvm64_batch_normal_range",
     "hvm64_server_create", "hvm64_server_submit", "hvm64_server_poll", "hvm64_server_result", "hvm64_server_free",
-    "hvm64_server_submit_nodes", "hvm64_server_budget",
+    "hvm64_server_submit_nodes", "hvm64_server_budget", "hvm64_pre_reduce", "hvm64_book_format",
 )
 
 
@@ -123,6 +124,10 @@ def lib(build_if_missing=True):
     L.hvm64_server_result.argtypes = [P, c.c_uint64, c.POINTER(Rewrites), c.POINTER(c.c_int),
                                       c.POINTER(c.c_double), c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_server_free.argtypes = [P]
+    L.hvm64_pre_reduce.argtypes = [c.c_char_p, c.c_size_t, c.c_char_p, c.c_uint64, c.c_uint64, c.POINTER(Tuning),
+                                   c.POINTER(Rewrites), c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_char_p,
+                                   c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_book_format.argtypes = [c.c_char_p, c.c_size_t, c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
     _lib = L
     return L
 
@@ -299,6 +304,34 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def book_format(text):
+    """ast::Book::from_str + Display: the Book as the reference prints it
+    (host-only; no device work)."""
+    data = text.encode()
+    return _read_text(lib().hvm64_book_format, data, len(data))
+
+
+def pre_reduce(text, skip=(), max_rwts=(1 << 64) - 1, heap_bytes=0, tuning=None):
+    """Book::pre_reduce (transform/src/pre_reduce.rs:27-74) on the GPU: every
+    Def not in `skip` is reduced (no expansion) and replaced by its result.
+    Returns (pre-reduced Book text, Rewrites, names of the Defs that did not
+    reach normal form within max_rwts popped redexes)."""
+    L = lib()
+    data = text.encode()
+    sk = " ".join(skip).encode()
+    rw = Rewrites()
+    n, nn = ctypes.c_size_t(), ctypes.c_size_t()
+    t = ctypes.byref(tuning) if tuning is not None else None
+    cap, ncap = max(8 * len(data), 1 << 16), max(len(data), 1 << 12)
+    while True:
+        buf, nbuf = ctypes.create_string_buffer(cap), ctypes.create_string_buffer(ncap)
+        _check(L.hvm64_pre_reduce(data, len(data), sk, max_rwts, heap_bytes, t, ctypes.byref(rw), buf, cap,
+                                  ctypes.byref(n), nbuf, ncap, ctypes.byref(nn)))
+        if n.value < cap and nn.value < ncap:
+            return buf.value.decode(), rw, [x for x in nbuf.value.decode().split("\n") if x]
+        cap, ncap = n.value + 1, nn.value + 1  # rare: the results outgrew the buffers
 
 
 def normal_noalloc(book, entry="main", tuning=None, cap=1 << 20):

@@ -43,6 +43,7 @@ extern "C" {
 #define HVM64_ERR_QUEUE 7     /* the device redex queue overflowed */
 #define HVM64_ERR_BAD_ADDR 8  /* a heap address outside the arena (internal fault, caught) */
 #define HVM64_ERR_OUTPUT 9    /* a served net's normal form did not fit its output buffer */
+#define HVM64_ERR_LIMIT 10    /* a run passed its interaction limit (pre-reduce's max_rwts) */
 
 /* Per-rule interaction counters: runtime/src/runtime.rs:72-79 (Rewrites). */
 typedef struct hvm64_rewrites {
@@ -136,6 +137,27 @@ typedef struct hvm64_stats {
 } hvm64_stats;
 int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
 int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
+
+/* ast::Book::from_str + Display (ast/src/parser.rs, ast/src/ast.rs:221-232):
+ * `book_text` as the reference prints a parsed Book.  References need not
+ * resolve.  Buffer convention as hvm64_net_readback. */
+int hvm64_book_format(const char* book_text, size_t len, char* buf, size_t cap, size_t* out_len);
+/* Book::pre_reduce (transform/src/pre_reduce.rs:27-74, as `hvm64 transform
+ * -O pre-reduce` runs it from src/main.rs:100-126) on the current device.
+ * `book_text` may reference Defs it lacks; those become inert Defs whose
+ * calls are kept as redexes.  Every Def not named in `skip` (names separated
+ * by spaces or newlines; nullable) is booted without the expansion agent and
+ * reduced, Defs it references first, one launch per Def on one heap of
+ * `heap_bytes` (0: a default); the result replaces the Def.  `out` receives
+ * the summed Rewrites, `buf` the pre-reduced Book's text (ast/src/ast.rs:
+ * 221-232 Display) and `not_normal` the names, one per line, of Defs whose
+ * reduction took `max_rwts` pops or more (UINT64_MAX: no limit).  Those keep
+ * their original net and add no Rewrites, where the reference keeps the net
+ * as it stood after max_rwts pops.  Buffers follow hvm64_net_readback's
+ * convention (cap = 0 sizes them). */
+int hvm64_pre_reduce(const char* book_text, size_t len, const char* skip, uint64_t max_rwts, uint64_t heap_bytes,
+                     const hvm64_tuning* tuning, hvm64_rewrites* out, char* buf, size_t cap, size_t* out_len,
+                     char* not_normal, size_t nn_cap, size_t* nn_len);
 
 /* Serving: one reducer that stays on the device and admits requests while it
  * runs (continuous batching).  No reference counterpart: the reference reduces

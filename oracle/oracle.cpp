@@ -26,6 +26,7 @@
 #include <deque>
 #include <functional>
 #include <map>
+#include <set>
 #include <memory>
 #include <optional>
 #include <pthread.h>
@@ -773,7 +774,9 @@ struct Instruction {
 };
 
 struct Net;
-enum DefKind : u8 { D_INTERPRETED, D_EXPAND };
+// D_INERT: transform/src/pre_reduce.rs:89-102 (InertDef), the stand-in for a
+// reference missing from a Book being pre-reduced; its calls are captured.
+enum DefKind : u8 { D_INTERPRETED, D_EXPAND, D_INERT };
 // def.rs:86-95; aligned so that Ref ports can address it.
 struct alignas(32) Def {
   LabSet labs;
@@ -843,6 +846,7 @@ struct Net {
   int order = 0;
   std::mt19937_64 rng{12345};
   size_t fifo_pos_fast = 0, fifo_pos_slow = 0;
+  std::vector<std::pair<u64, u64>>* captured = nullptr;  // InertDef calls (pre-reduce)
 
   Net(u64 base, size_t nodes) : heap_base(base), heap_nodes(nodes), trgs(1 << 16) {}
 
@@ -1101,7 +1105,10 @@ struct Net {
     if (ptag(trg) == Ctr && !def->labs.has(plab(trg))) return comm02(port, trg);
     rwts.dref++;
     if (def->kind == D_EXPAND) expand_call(def, trg);
-    else interpreted_call(def, trg);
+    else if (def->kind == D_INERT) {  // pre_reduce.rs:96-101
+      if (!captured) throw Panic(E_BAD_INPUT, "inert definition called outside pre-reduce");
+      captured->push_back({port_ref(def), trg});
+    } else interpreted_call(def, trg);
   }
 
   // ---- instruction.rs:403-500
@@ -1474,11 +1481,19 @@ struct Host {
     back[paddr(port_ref(d.get()))] = name;
     defs[name] = std::move(d);
   }
-  void insert_book(const Book& b) {
+  // host.rs:34-73.  With `inert_missing` (insert_book_with_default as
+  // pre_reduce.rs:41 calls it) a reference the Book lacks becomes an inert def
+  // with LabSet::ALL.
+  void insert_book(const Book& b, bool inert_missing = false) {
     auto sets = calculate_label_sets(b, [&](const std::string& name) -> LabSet {
       auto it = defs.find(name);
       if (it != defs.end()) return it->second->labs;
-      throw Panic(E_BAD_INPUT, "Found reference \"" + name + "\", which is not in the book!");
+      if (!inert_missing) throw Panic(E_BAD_INPUT, "Found reference \"" + name + "\", which is not in the book!");
+      auto d = std::make_unique<Def>();
+      d->labs = LabSet::all();
+      d->kind = D_INERT;
+      insert_def(name, std::move(d));
+      return defs[name]->labs;
     });
     for (auto& [name, labs] : sets) {
       auto d = std::make_unique<Def>();
@@ -1821,6 +1836,81 @@ static RunResult run_expr(Host& host, const AstNet& expr, int mode, int threads,
   return rr;
 }
 
+// transform/src/pre_reduce.rs:38-74,136-164.  Every def of the Book not
+// skipped is visited in byte order of names; a def first pre-reduces the defs
+// its (original) net references, depth first (a def met again while still on
+// the path is left as it is: the "Cycled" state).  Then it is booted in a
+// fresh Net on the shared heap without the expansion agent and reduced with
+// `Net::reduce(max_rwts)`; redexes captured by inert defs go back into the
+// net's redex queue; the read-back net replaces the def's instructions at once
+// (so later defs call the reduced version) and, at the end, its text in the
+// Book.  Label sets stay those of the original Book.
+struct PreReducer {
+  Host& host;
+  Heap& heap;
+  const std::set<std::string>& skip;
+  u64 max_rwts;
+  Arena arena;
+  std::vector<std::pair<u64, u64>> captured;
+  std::map<std::string, int> seen;  // 0: on the path (Cycled), 1: reduced
+  std::map<std::string, std::pair<AstNet, bool>> reduced;  // net, reached normal form
+  Rewrites rw;
+
+  void visit_tree(const Tree* t) {  // pre_reduce.rs:122-129
+    if (t->kind == T_REF) pre_reduce(t->name);
+    if (t->p1) visit_tree(t->p1);
+    if (t->p2) visit_tree(t->p2);
+  }
+  void pre_reduce(const std::string& name) {  // pre_reduce.rs:137-164
+    if (seen.count(name) || skip.count(name) || !host.book.nets.count(name)) return;
+    seen[name] = 0;
+    const AstNet& src = host.book.nets.at(name);
+    visit_tree(src.root);
+    for (auto& r : src.redexes) {
+      visit_tree(r.first);
+      visit_tree(r.second);
+    }
+    auto rt = net_new(heap);
+    rt->captured = &captured;
+    rt->boot(host.defs.at(name).get());
+    bool normal = rt->reduce(max_rwts > u64(SIZE_MAX) ? SIZE_MAX : size_t(max_rwts));
+    rw.anni += rt->rwts.anni; rw.comm += rt->rwts.comm; rw.eras += rt->rwts.eras;
+    rw.dref += rt->rwts.dref; rw.oper += rt->rwts.oper;
+    for (auto& [a, b] : captured) rt->redux(a, b);
+    captured.clear();
+    AstNet net = host.readback(*rt, arena, false);
+    host.encode_def(net, *host.defs.at(name));
+    seen[name] = 1;
+    reduced[name] = {net, normal};
+  }
+};
+
+struct PreReduceResult {
+  std::string text;
+  Rewrites rw;
+  std::vector<std::string> not_normal;
+};
+
+static PreReduceResult pre_reduce_book(const std::string& text, const std::set<std::string>& skip, u64 max_rwts,
+                                       size_t heap_bytes) {
+  PreReduceResult out;
+  with_big_stack([&] {
+    Host host;
+    host.book = parse_book(text);
+    host.insert_book(host.book, true);
+    Heap heap(heap_bytes ? heap_bytes : default_heap_bytes());
+    PreReducer p{host, heap, skip, max_rwts, {}, {}, {}, {}, {}};
+    for (auto& [name, _] : host.book.nets) p.pre_reduce(name);
+    for (auto& [name, st] : p.reduced) {  // pre_reduce.rs:60-67
+      host.book.nets[name] = st.first;
+      if (!st.second) out.not_normal.push_back(name);
+    }
+    out.rw = p.rw;
+    out.text = book_to_string(host.book);
+  });
+  return out;
+}
+
 }  // namespace hvo
 
 // ===========================================================================
@@ -1945,6 +2035,31 @@ int hvo_book_apply(const char* text, const char* def_name, const char* arg_tree,
 int hvo_book_roundtrip(const char* text, char** out_text) {
   return guarded([&] {
     with_big_stack([&] { *out_text = dupstr(book_to_string(parse_book(text))); });
+  });
+}
+
+// Book::pre_reduce (transform/src/pre_reduce.rs:27-74): `skip` holds the
+// '\n'-separated names not to pre-reduce.  Returns the pre-reduced Book's text
+// (ast.rs Display), rw[0..5] and the '\n'-separated names of the defs whose
+// reduction stopped at `max_rwts`.
+int hvo_pre_reduce(const char* text, const char* skip, uint64_t max_rwts, uint64_t heap_bytes, char** out_text,
+                   uint64_t* rw, char** out_not_normal) {
+  return guarded([&] {
+    std::set<std::string> sk;
+    std::string a = skip ? skip : "";
+    size_t s = 0;
+    while (s < a.size()) {
+      size_t e = a.find('\n', s);
+      if (e == std::string::npos) e = a.size();
+      if (e > s) sk.insert(a.substr(s, e - s));
+      s = e + 1;
+    }
+    PreReduceResult r = pre_reduce_book(text, sk, max_rwts, heap_bytes);
+    *out_text = dupstr(r.text);
+    rw[0] = r.rw.anni; rw[1] = r.rw.comm; rw[2] = r.rw.eras; rw[3] = r.rw.dref; rw[4] = r.rw.oper;
+    std::string nn;
+    for (auto& n : r.not_normal) nn += n + "\n";
+    *out_not_normal = dupstr(nn);
   });
 }
 

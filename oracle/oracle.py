@@ -51,6 +51,8 @@ def lib():
         L.hvo_num_print.argtypes = [c.c_uint32, c.POINTER(c.c_void_p)]
         L.hvo_num_f24.argtypes = [c.c_float]
         L.hvo_num_f24.restype = c.c_uint32
+        L.hvo_pre_reduce.argtypes = [c.c_char_p, c.c_char_p, c.c_uint64, c.c_uint64, c.POINTER(c.c_void_p),
+                                     c.POINTER(c.c_uint64), c.POINTER(c.c_void_p)]
         _lib = L
     return _lib
 
@@ -84,6 +86,17 @@ def run_book(text, entry="main", mode=MODE_NORMAL, threads=0, seed=7, heap_bytes
     _check(lib().hvo_run_book(text.encode(), entry.encode(), mode, threads, seed, heap_bytes, int(resolve),
                               ctypes.byref(out), rw, ctypes.byref(sec)))
     return _take(out), dict(zip(COUNT_KEYS, list(rw))), sec.value
+
+
+def pre_reduce(text, skip=("main",), max_rwts=(1 << 64) - 1, heap_bytes=0):
+    """Book::pre_reduce (transform/src/pre_reduce.rs:27-74) with the names in
+    `skip` left as they are.  Returns (pre-reduced Book text, {anni, comm,
+    eras, dref, oper}, names of defs that stopped at max_rwts)."""
+    out, nn = ctypes.c_void_p(), ctypes.c_void_p()
+    rw = (ctypes.c_uint64 * 5)()
+    _check(lib().hvo_pre_reduce(text.encode(), "\n".join(skip).encode(), max_rwts, heap_bytes, ctypes.byref(out),
+                                rw, ctypes.byref(nn)))
+    return _take(out), dict(zip(COUNT_KEYS, rw)), [n for n in _take(nn).split("\n") if n]
 
 
 def run_expr(book_text, expr, mode=MODE_NORMAL, threads=0, heap_bytes=0):

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <set>
 #include <string>
 #include <memory>
 #include <thread>
@@ -83,6 +84,7 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsig
   Ctx c{W.get(), 0, 0};
   unsigned top = 0, bot = 0;
   int cur = -1;
+  ull pops = 0;  // redexes this lane interacted (Net::reduce's count)
   for (;;) {
     if (ld_gpu32(&E->C.error)) break;
     if (W->sp_n && top - bot < 4) {  // refill from the overflow stack's newest
@@ -133,6 +135,7 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsig
     W->ring_base = top;
     W->ring_cap = std::min(unsigned(SCAP) - (top - bot), ring);
     interact(c, a, b);
+    pops++;
     settle(c);
     {
       unsigned cnt = W->ring_cnt;
@@ -165,6 +168,67 @@ void worker(Emu* E, unsigned share_min, unsigned ring, unsigned spill_cap, unsig
     }
   }
   if (cur >= 0) flush(*W, E->nets[cur]);
+  atom_add(&E->C.stat_lanes, pops);
+}
+
+// Boots Def `prog` of `book` in a fresh emulated device and reduces it on
+// `threads` host threads.  With `capture` (pre-reduce), the boot skips the
+// expansion agent and inert Defs record their redexes there.
+std::unique_ptr<Emu> emu_reduce(const Book& book, uint32_t prog, unsigned threads, unsigned ring,
+                                unsigned spill_cap, unsigned share_min, uint64_t heap_bytes, uint64_t chunk,
+                                std::vector<ull>* capture) {
+  auto Ep = std::make_unique<Emu>();
+  Emu& E = *Ep;
+  E.heap.assign(heap_bytes / 8, 0);
+  E.nets.assign(1, NetState{});
+  E.nets[0].prog = int(prog);
+  E.C.bump = 1;
+  E.C.heap_nodes = heap_bytes / 16;
+  E.C.heap_bytes = heap_bytes;
+  E.C.chunk_nodes = chunk;
+  E.C.reuse_mark = 0;  // free nodes shared between threads from the start
+  E.C.spin_limit = 1ull << 26;
+  E.C.deadline = globaltimer() + 120ull * 1000000000ull;
+  E.P.heap = E.heap.data();
+  E.P.heap_bytes = heap_bytes;
+  E.P.ctrl = &E.C;
+  E.P.nets = E.nets.data();
+  E.P.nnets = 1;
+  E.P.defs = book.defs.data();
+  E.P.instrs = book.instrs.data();
+  E.P.labbits = reinterpret_cast<const ull*>(book.labbits.data());
+  E.P.ndefs = unsigned(book.defs.size());
+  E.P.ovf_flush = OVF_FLUSH;
+  if (capture) {
+    E.P.no_expand = 1;
+    E.P.capture = capture->data();
+    E.P.capture_cap = unsigned(capture->size() / 2);
+  }
+  g_P = E.P;
+  // boot (the boot kernel's steps, one thread)
+  g_emu = &E;
+  {
+    auto W = new_warp();
+    std::vector<ull> boot_regs(32 * MAX_REGS);
+    W->bigregs = boot_regs.data();
+    W->ring_cap = 0;  // boot redexes go straight to the shared queue
+    Ctx c{W.get(), 0, 0};
+    ull root = alloc(c);
+    if (!(book.defs[prog].flags & DEF_EXPR)) W->rw[RW_DREF]++;
+    run_def(c, prog, pvar(root));
+    settle(c);
+    if (!g_P.no_expand) {
+      root = expand(c, root);
+      settle(c);
+    }
+    E.nets[0].root = root;
+    flush(*W, E.nets[0]);
+    if (E.nets[0].pending > 0) E.C.nets_left = 1;
+  }
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min, std::max(1u, ring), spill_cap, t);
+  for (auto& t : th) t.join();
+  return Ep;
 }
 }  // namespace
 
@@ -185,49 +249,8 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
     with_big_stack([&] { book.load(parse_book(src)); });
     auto it = book.ids.find(entry);
     if (it == book.ids.end()) throw Error(HVM64_ERR_BAD_INPUT, "no entry");
-    Emu E;
-    E.heap.assign(heap_bytes / 8, 0);
-    E.nets.assign(1, NetState{});
-    E.nets[0].prog = int(it->second);
-    E.C.bump = 1;
-    E.C.heap_nodes = heap_bytes / 16;
-    E.C.heap_bytes = heap_bytes;
-    E.C.chunk_nodes = chunk;
-    E.C.reuse_mark = 0;  // free nodes shared between threads from the start
-    E.C.spin_limit = 1ull << 26;
-    E.C.deadline = globaltimer() + 120ull * 1000000000ull;
-    E.P.heap = E.heap.data();
-    E.P.heap_bytes = heap_bytes;
-    E.P.ctrl = &E.C;
-    E.P.nets = E.nets.data();
-    E.P.nnets = 1;
-    E.P.defs = book.defs.data();
-    E.P.instrs = book.instrs.data();
-    E.P.labbits = reinterpret_cast<const ull*>(book.labbits.data());
-    E.P.ndefs = unsigned(book.defs.size());
-    E.P.ovf_flush = OVF_FLUSH;
-    g_P = E.P;
-    // boot (the boot kernel's steps, one thread)
-    g_emu = &E;
-    {
-      auto W = new_warp();
-      std::vector<ull> boot_regs(32 * MAX_REGS);
-      W->bigregs = boot_regs.data();
-      W->ring_cap = 0;  // boot redexes go straight to the shared queue
-      Ctx c{W.get(), 0, 0};
-      ull root = alloc(c);
-      if (!(book.defs[it->second].flags & 1)) W->rw[RW_DREF]++;
-      run_def(c, it->second, pvar(root));
-      settle(c);
-      root = expand(c, root);
-      settle(c);
-      E.nets[0].root = root;
-      flush(*W, E.nets[0]);
-      if (E.nets[0].pending > 0) E.C.nets_left = 1;
-    }
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < threads; t++) th.emplace_back(worker, &E, share_min, std::max(1u, ring), spill_cap, t);
-    for (auto& t : th) t.join();
+    auto Ep = emu_reduce(book, it->second, threads, ring, spill_cap, share_min, heap_bytes, chunk, nullptr);
+    Emu& E = *Ep;
     if (E.C.error) {
       snprintf(err, errcap, "device error %d info 0x%llx", E.C.error, (unsigned long long)E.C.error_info);
       return E.C.error;
@@ -272,6 +295,70 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
       }
     }
     *out_text = strdup(txt.c_str());
+    return 0;
+  } catch (Error& e) {
+    snprintf(err, errcap, "%s", e.msg.c_str());
+    return e.code;
+  } catch (std::exception& e) {
+    snprintf(err, errcap, "%s", e.what());
+    return HVM64_ERR_BAD_INPUT;
+  }
+}
+
+// Book::pre_reduce with every Def reduced by the emulated device (the same
+// host driver, hvm::pre_reduce, that the CUDA library uses).  `skip` holds
+// '\n'-separated names; rw[0..5]; not_normal gets one name per line.
+extern "C" int hvm64emu_pre_reduce(const char* book_text, const char* skip, uint64_t max_rwts, unsigned threads,
+                                   unsigned ring, unsigned spill_cap, uint64_t heap_bytes, uint64_t chunk,
+                                   char** out_text, uint64_t* rw, char** not_normal, char* err, size_t errcap) {
+  try {
+    AstBook ast;
+    Book book;
+    std::string src(book_text);
+    with_big_stack([&] {
+      ast = parse_book(src);
+      book.load(ast, true);
+    });
+    std::set<std::string> sk;
+    std::string names = skip ? skip : "";
+    for (size_t s0 = 0; s0 < names.size();) {
+      size_t e = names.find('\n', s0);
+      if (e == std::string::npos) e = names.size();
+      if (e > s0) sk.insert(names.substr(s0, e - s0));
+      s0 = e + 1;
+    }
+    PreReduceOut res;
+    with_big_stack([&] {
+      res = pre_reduce(ast, book, sk, max_rwts, [&](uint32_t id) {
+        std::vector<ull> cap(2 * 4096);
+        auto E = emu_reduce(book, id, threads, ring, spill_cap, 16, heap_bytes, chunk, &cap);
+        PreReduceRun r;
+        r.status = E->C.error;
+        r.pops = E->C.stat_lanes;
+        for (int k = 0; k < 5; k++) r.rw[k] = E->nets[0].rw[k];
+        if (r.status) {
+          r.error = "device error " + std::to_string(r.status);
+          return r;
+        }
+        // captured redexes after the net's own, ones with an eraser first
+        std::vector<uint64_t> pairs;
+        uint64_t n = std::min<uint64_t>(E->C.captured, cap.size() / 2);
+        for (int pass = 0; pass < 2; pass++)
+          for (uint64_t k = 0; k < n; k++)
+            if ((cap[2 * k + 1] == PORT_ERA) == (pass == 0)) {
+              pairs.push_back(cap[2 * k]);
+              pairs.push_back(cap[2 * k + 1]);
+            }
+        r.text = readback_net(book, reinterpret_cast<const uint64_t*>(E->heap.data()), E->heap.size(),
+                              E->nets[0].root, pairs.data(), pairs.size() / 2);
+        return r;
+      });
+    });
+    for (int k = 0; k < 5; k++) rw[k] = res.rw[k];
+    *out_text = strdup(res.text.c_str());
+    std::string nn;
+    for (auto& n : res.not_normal) nn += n + "\n";
+    *not_normal = strdup(nn.c_str());
     return 0;
   } catch (Error& e) {
     snprintf(err, errcap, "%s", e.msg.c_str());

@@ -11,6 +11,9 @@ It reads, as text, and writes under tests/golden/:
   lists.json      tests/lists.rs: list_put_got.hvm and the pinned RWTS totals
   cli.json        tests/cli.rs: `reduce`/`run` outputs and apply_tree cases
   labels.json     host/src/calc_labels.rs:196-234 label-set expectations
+  pre_reduce.json tests/snapshots/pre_reduce_run@<name>.snap (pre-reduce then
+                  run)
+  transform.json  tests/transform.rs: per-rule counts of pre-reduce + run
 
 Nothing at test time reads the reference checkout; only these fixtures.
 """
@@ -66,6 +69,47 @@ def programs(ref):
     return out
 
 
+def pre_reduce(ref):
+    """tests/tests.rs:44-55: each program pre-reduced (`main` skipped, no
+    rewrite limit) then run: `pre_reduce_run@<name>.snap` holds the normal
+    form, the pre-reduce Rewrites and the run's Rewrites."""
+    progs = []
+    for p in programs(ref):
+        snap = os.path.join(ref, "tests/snapshots", f"pre_reduce_run@{p['name']}.snap")
+        if not os.path.exists(snap):
+            continue
+        body = snap_body(snap).rstrip("\n").split("\n")
+        if "pre-reduce:" in body:
+            i, j = body.index("pre-reduce:"), body.index("run:")
+            text, pre, run = "\n".join(body[:i]), parse_counts(body[i + 1:j]), parse_counts(body[j + 1:])
+        else:  # no run (tests.rs:47-50): only the pre-reduce Rewrites
+            text, pre, run = None, parse_counts(body), None
+        progs.append({"name": p["name"], "source": p["source"], "text": text, "pre": pre, "run": run})
+    return progs
+
+
+def transform(ref):
+    """tests/transform.rs:14-47 (test_fast_pre_reduce): heavy_pre_reduction.hvm
+    without `black_box` is pre-reduced keeping only the listed defs' reduction
+    (every other def is skipped), `black_box` is put back, the entry is run
+    with normal(), and the pre-reduce plus run counts are pinned."""
+    src = open(os.path.join(ref, "tests/transform.rs")).read()
+    body = src[src.index("fn test_fast_pre_reduce"):]
+    lists = re.findall(r"!\[([^\]]*)\]\.contains", body)[:2]
+    only = [re.findall(r'"(\w+)"', x) for x in lists]
+    snap = re.search(r'@r###"(.*?)"###', body, re.S).group(1)
+    lines = [ln.strip() for ln in snap.strip("\n").split("\n")]
+    i = lines.index("Slow:")
+    return {
+        "source": open(os.path.join(ref, "tests/programs/heavy_pre_reduction.hvm")).read(),
+        "removed": "black_box",
+        "cases": [
+            {"only": only[0], "entry": "main_fast", "total": parse_counts(lines[1:i])},
+            {"only": only[1], "entry": "main_slow", "total": parse_counts(lines[i + 1:])},
+        ],
+    }
+
+
 def lists(ref):
     src = open(os.path.join(ref, "tests/lists.rs")).read()
     got_idx = [int(x) for x in re.search(r"for index in \[([^\]]*)\]", src).group(1).split(",")]
@@ -117,7 +161,8 @@ def main():
         sys.exit("usage: make_golden.py <reference checkout>")
     here = os.path.dirname(os.path.abspath(__file__))
     for fname, data in (("programs.json", programs(ref)), ("lists.json", lists(ref)),
-                        ("cli.json", cli(ref)), ("labels.json", labels(ref))):
+                        ("cli.json", cli(ref)), ("labels.json", labels(ref)),
+                        ("pre_reduce.json", pre_reduce(ref)), ("transform.json", transform(ref))):
         with open(os.path.join(here, fname), "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)
             f.write("\n")
