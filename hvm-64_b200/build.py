@@ -61,6 +61,43 @@ def build(force=False, verbose=False):
     return LIB
 
 
+GEN = os.path.join(OUT, "gen")
+
+
+def compiled_source_hash(source):
+    """The Book hash a generated source was made for (its HVM_GEN_HASH)."""
+    for line in source.splitlines():
+        if line.startswith("#define HVM_GEN_HASH "):
+            return line.split()[2].removesuffix("ull")
+    raise ValueError("not a generated Def source")
+
+
+def build_compiled(source, verbose=False):
+    """`hvm64 compile` for a Book: `source` is its generated Def functions
+    (hvm64.Book.compile_source, hvm64_book_compile_source).  Builds
+    build/gen/libhvm64_<hash>.so, the reducer library with those functions in
+    place of the instruction VM for that Book (any other Book still runs on
+    the VM), and returns its path.  Rebuilt only when missing or stale."""
+    build()
+    os.makedirs(GEN, exist_ok=True)
+    h = compiled_source_hash(source)
+    hdr = os.path.join(GEN, f"defs_{h}.cuh")
+    lib = os.path.join(GEN, f"libhvm64_{h}.so")
+    if not os.path.exists(hdr) or open(hdr).read() != source:
+        with open(hdr, "w") as f:
+            f.write(source)
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(INC, "hvm64.h"), hdr, __file__]
+    if _stale(lib, deps):
+        obj = os.path.join(GEN, f"hvm64_{h}.o")
+        log = _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xptxas", "-v",
+                    "-Xcompiler", "-fPIC", "-I", INC, f'-DHVM_GEN_INCLUDE="{hdr}"', "-c",
+                    os.path.join(CSRC, "hvm64.cu"), "-o", obj])
+        if verbose:
+            sys.stderr.write(log)
+        _run([NVCC, *ARCH, "-shared", "-o", lib, obj, os.path.join(OUT, "host.o"), "-lcudart"])
+    return lib
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     print(LIB)

@@ -165,6 +165,7 @@ struct Params {
   unsigned no_expand, capture_cap;
   ull* capture;
   ull rw_limit;
+  unsigned gen;  // 1: the compiled Def functions match the loaded Book (HVM_GEN_INCLUDE builds)
   // serving (all zero for a batch run)
   unsigned serve;
   const ServeReq* req;         // device ring of req_cap requests
@@ -1066,9 +1067,17 @@ HVM_COLD void exec_large(const Ctx& c, const DevDef& d, ull t0) {
   if (!c.W->bigregs || d.nregs > MAX_REGS) return run_fail(c.net, HVM64_ERR_BAD_INPUT, d.nregs);
   exec(c, d, t0, c.W->bigregs + c.lane, 32, g_P.instrs + d.ins_off);
 }
+// A compiled build (hvm64 compile) includes the Book's Defs as functions;
+// they run when the loaded Book is the one they were generated from.
+#ifdef HVM_GEN_INCLUDE
+#include HVM_GEN_INCLUDE
+#endif
 HVM_COLD void run_def(const Ctx& c, unsigned id, ull t0) {
   PROF_RULE(5)
   if (id >= g_P.ndefs) return run_fail(c.net, HVM64_ERR_BAD_INPUT, id);
+#ifdef HVM_GEN_INCLUDE
+  if (g_P.gen && gen_call(c, id, t0)) return;
+#endif
   ull* R = c.W->regs + c.lane;
   if (id == c.W->icache_def) {  // staged by the warp for this step
     const DevDef& d = c.W->idef;

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <charconv>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <optional>
@@ -865,6 +866,93 @@ std::string readback(const Book& book, const uint64_t* heap, uint64_t heap_words
   Reader r{book, heap, heap_words, {}, 0, {}};
   r.wire(root);
   return r.o;
+}
+
+// ===========================================================================
+// Ahead-of-time Def specialisation (src/compile.rs:110-161)
+// ===========================================================================
+uint64_t defs_hash(const Book& book, uint32_t n) {
+  // FNV-1a over every field the generated code or its dispatch depends on
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto mix = [&](uint64_t v) {
+    for (int k = 0; k < 8; k++) {
+      h ^= (v >> (8 * k)) & 0xff;
+      h *= 0x100000001b3ull;
+    }
+  };
+  mix(n);
+  for (uint32_t id = 0; id < n && id < book.defs.size(); id++) {
+    const DevDef& d = book.defs[id];
+    mix(d.ins_len);
+    mix(d.nregs);
+    mix(d.min_safe);
+    mix(d.flags);
+    mix(d.nodes);
+    mix(d.redexes);
+    for (uint32_t k = 0; k < d.lab_len; k++) mix(book.labbits[d.lab_off + k]);
+    for (uint32_t k = 0; k < d.ins_len; k++) {
+      const DevInstr& x = book.instrs[d.ins_off + k];
+      mix(uint64_t(x.k) | uint64_t(x.op) << 8 | uint64_t(x.lab) << 16 | uint64_t(x.a) << 32 | uint64_t(x.b) << 40 |
+          uint64_t(x.c) << 48 | uint64_t(x.d) << 56);
+      mix(x.port);
+    }
+  }
+  return h;
+}
+
+std::string compile_defs_cuda(const Book& book) {
+  const uint32_t n = book.def_count();
+  char buf[256];
+  std::string o;
+  snprintf(buf, sizeof buf, "// Generated by hvm64 compile: %u definitions.\n#define HVM_GEN_NDEFS %uu\n"
+           "#define HVM_GEN_HASH 0x%016llxull\n\n", n, n, (unsigned long long)defs_hash(book, n));
+  o += buf;
+  auto hex = [&](uint64_t v) {
+    snprintf(buf, sizeof buf, "0x%llxull", (unsigned long long)v);
+    return std::string(buf);
+  };
+  auto r = [](unsigned i) { return "r" + std::to_string(i); };
+  for (uint32_t id = 0; id < n; id++) {
+    const DevDef& d = book.defs[id];
+    o += "// @" + book.names[id] + "\n";
+    o += "HVM_COLD void gen_def_" + std::to_string(id) + "(const Ctx& c, ull r0) {\n";
+    if (d.nregs > 1) {
+      o += "  ull";
+      for (uint32_t k = 1; k < d.nregs; k++) o += (k > 1 ? ", " : " ") + r(k);
+      o += ";\n";
+    }
+    for (uint32_t k = 0; k < d.ins_len; k++) {
+      const DevInstr& x = book.instrs[d.ins_off + k];
+      switch (x.k) {
+        case I_CONST: o += "  " + r(x.a) + " = " + hex(x.port) + ";\n"; break;
+        case I_LINK: o += "  count(c, EX_DLINKS); link_trg(c, " + r(x.a) + ", " + r(x.b) + ");\n"; break;
+        case I_LINKCONST: o += "  count(c, EX_DLINKS); link_trg_port(c, " + r(x.a) + ", " + hex(x.port) + ");\n"; break;
+        case I_CTR:
+          o += "  do_ctr(c, " + std::to_string(x.lab) + "u, " + r(x.a) + ", " + r(x.b) + ", " + r(x.c) + ");\n";
+          break;
+        case I_OP:
+          o += "  do_op(c, " + std::to_string(x.op) + "u, " + r(x.a) + ", " + r(x.b) + ", " + r(x.c) + ");\n";
+          break;
+        case I_OPNUM:
+          o += "  " + r(x.c) + " = do_op_num(c, " + std::to_string(x.op) + "u, " + r(x.a) + ", " +
+               std::to_string(uint32_t(x.port)) + "u);\n";
+          break;
+        case I_SWITCH: o += "  do_switch(c, " + r(x.a) + ", " + r(x.b) + ", " + r(x.c) + ");\n"; break;
+        case I_WIRES:
+          o += "  { ull n = alloc(c); " + r(x.a) + " = pvar(n); " + r(x.b) + " = n; " + r(x.c) + " = pvar(n ^ 8); " +
+               r(x.d) + " = n ^ 8; }\n";
+          break;
+        case I_CAPTURE: o += "  capture(c, " + hex(x.port) + ", " + r(x.a) + ");\n"; break;
+      }
+    }
+    o += "}\n";
+  }
+  o += "\n// The Def's function for Def `id` (false: none; the VM runs it).\n";
+  o += "HVM_INL bool gen_call(const Ctx& c, unsigned id, ull t0) {\n  switch (id) {\n";
+  for (uint32_t id = 0; id < n; id++)
+    o += "    case " + std::to_string(id) + "u: gen_def_" + std::to_string(id) + "(c, t0); return true;\n";
+  o += "  }\n  return false;\n}\n";
+  return o;
 }
 
 // ===========================================================================

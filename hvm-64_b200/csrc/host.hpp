@@ -197,6 +197,18 @@ struct PreReduceOut {
 PreReduceOut pre_reduce(const AstBook& ast, Book& book, const std::set<std::string>& skip, uint64_t max_rwts,
                         const std::function<PreReduceRun(uint32_t)>& run_one);
 
+// Ahead-of-time Def specialisation (the analogue of `hvm64 compile`,
+// src/compile.rs:110-161): CUDA source with one straight-line function per
+// Def of `book` (its instructions as direct calls on registers held in
+// variables, instead of the device VM's loop over an instruction table) and
+// the dispatch `gen_call`; included into the device runtime it replaces the
+// VM for Books whose device tables hash to the same value.
+std::string compile_defs_cuda(const Book& book);
+// Hash of the device tables of Defs [0, n) (instructions, register counts,
+// labels, flags): a compiled build runs its functions only for a Book whose
+// hash matches the one it was generated from.
+uint64_t defs_hash(const Book& book, uint32_t n);
+
 // Runs f on a thread with a large stack (deep trees recurse; the reference
 // grows its stack with `stacker`, util/src/maybe_grow.rs).
 void with_big_stack(const std::function<void()>& f);

@@ -640,7 +640,12 @@ __global__ void __launch_bounds__(THREADS, HVM_MINB) reduce_kernel() {
     __syncwarp();
     const unsigned staged = W.icache_def;
     __syncwarp();
-    if (key >= 64u && key - 64u < g_P.ndefs && key - 64u != staged) {
+#ifdef HVM_GEN_INCLUDE
+    const bool vm_def = !(g_P.gen && key - 64u < HVM_GEN_NDEFS);  // compiled Defs need no staging
+#else
+    const bool vm_def = true;
+#endif
+    if (key >= 64u && key - 64u < g_P.ndefs && key - 64u != staged && vm_def) {
       unsigned id = key - 64u;
       const DevDef d = g_P.defs[id];
       if (d.ins_len <= ICACHE) {
@@ -881,6 +886,17 @@ const char* status_name(int s) {
   return "unknown error";
 }
 
+// Whether this build's compiled Def functions (hvm64 compile) are those of
+// `book`: 1 runs them, 0 the instruction VM.
+unsigned gen_matches(const Book& book) {
+#ifdef HVM_GEN_INCLUDE
+  return book.defs.size() >= HVM_GEN_NDEFS && defs_hash(book, HVM_GEN_NDEFS) == HVM_GEN_HASH ? 1u : 0u;
+#else
+  (void)book;
+  return 0u;
+#endif
+}
+
 // Resident reducer blocks per SM for a tuning (the occupancy limit when the
 // tuning leaves it at 0).
 int reducer_blocks_per_sm(const hvm64_tuning& t) {
@@ -1012,8 +1028,10 @@ struct Runner {
     if (heap_bytes < 64) throw Error(HVM64_ERR_BAD_INPUT, "heap too small");
   }
 
+  unsigned gen = 0;  // gen_matches(book), as of the last upload
   void upload_book() {
     if (uploaded_defs == book.defs.size() && d_defs.p) return;
+    gen = gen_matches(book);
     d_defs.alloc(book.defs.size());
     d_instrs.alloc(book.instrs.size());
     d_labbits.alloc(book.labbits.size());
@@ -1042,6 +1060,7 @@ struct Runner {
     p.spill_cap = spill_cap;
     p.ovf_flush = dev::OVF_FLUSH;
     p.bigregs = bigregs.p;
+    p.gen = gen;
     p.no_expand = no_expand ? 1u : 0u;
     p.rw_limit = rw_limit;
     p.capture = capture.p;
@@ -1634,6 +1653,7 @@ struct Server {
     // back while nothing is live (each lane's part-used chunk and unpublished
     // free list, each warp's reuse pool).
     p.ovf_flush = SERVE_OVF_FLUSH;
+    p.gen = gen_matches(book);
     const uint64_t reserve = warps * 32 * (c.chunk_nodes + SERVE_OVF_FLUSH) + warps * dev::POOL;
     if (heap_bytes / 16 <= 2 * reserve)
       throw Error(HVM64_ERR_BAD_INPUT, "heap_bytes too small for a server: its allocator may hold back " +
@@ -1964,6 +1984,12 @@ int hvm64_net_stats(const hvm64_net* n, hvm64_stats* out) {
   return HVM64_OK;
 }
 
+int hvm64_book_compile_source(const hvm64_book* book, char* buf, size_t cap, size_t* out_len) {
+  if (!book) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
+  return guarded([&] { copy_out(hvm::compile_defs_cuda(book->book), buf, cap, out_len); });
+}
+int hvm64_book_is_compiled(const hvm64_book* book) { return book ? int(hvm::gen_matches(book->book)) : 0; }
+
 int hvm64_book_format(const char* text, size_t len, char* buf, size_t cap, size_t* out_len) {
   if (!text) return hvm::set_error(HVM64_ERR_BAD_INPUT, "null argument");
   return guarded([&] {
@@ -2155,6 +2181,7 @@ std::string run(const Book& book, const char* name, const hvm64_tuning* tp, hvm6
   p.ndefs = unsigned(book.defs.size());
   p.spill = reinterpret_cast<dev::ull*>(base + OFF_SPILL);
   p.spill_cap = SPILL;
+  p.gen = gen_matches(book);
   p.ovf_flush = dev::OVF_FLUSH;
   hvm64_tuning tg = t;
   if (tg.blocks_per_sm == 0 || tg.blocks_per_sm > 4) tg.blocks_per_sm = 4;

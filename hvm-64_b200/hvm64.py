@@ -31,6 +31,7 @@ EXPORTS = (
     "hvm64_batch_normal_range",
     "hvm64_server_create", "hvm64_server_submit", "hvm64_server_poll", "hvm64_server_result", "hvm64_server_free",
     "hvm64_server_submit_nodes", "hvm64_server_budget", "hvm64_pre_reduce", "hvm64_book_format",
+    "hvm64_book_compile_source", "hvm64_book_is_compiled",
 )
 
 
@@ -128,6 +129,8 @@ def lib(build_if_missing=True):
                                    c.POINTER(Rewrites), c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_char_p,
                                    c.c_size_t, c.POINTER(c.c_size_t)]
     L.hvm64_book_format.argtypes = [c.c_char_p, c.c_size_t, c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_book_compile_source.argtypes = [P, c.c_char_p, c.c_size_t, c.POINTER(c.c_size_t)]
+    L.hvm64_book_is_compiled.argtypes = [P]
     _lib = L
     return L
 
@@ -157,6 +160,16 @@ class Book:
         data = text.encode()
         _check(lib().hvm64_book_load(data, len(data), ctypes.byref(h)))
         return cls(h)
+
+    def compile_source(self):
+        """CUDA source of this Book's Defs as straight-line device functions
+        (the analogue of `hvm64 compile`); build.build_compiled turns it into
+        a library."""
+        return _read_text(lib().hvm64_book_compile_source, self._h)
+
+    def is_compiled(self):
+        """True when the loaded library runs compiled functions for this Book."""
+        return bool(lib().hvm64_book_is_compiled(self._h))
 
     def names(self):
         L = lib()

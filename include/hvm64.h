@@ -138,6 +138,14 @@ typedef struct hvm64_stats {
 int hvm64_batch_stats(const hvm64_batch* batch, hvm64_stats* out);
 int hvm64_net_stats(const hvm64_net* net, hvm64_stats* out);
 
+/* `hvm64 compile` (src/compile.rs:110-161): CUDA source with one straight-line
+ * device function per Def of `book` and their dispatch.  A library built with
+ * it (hvm-64_b200/build.py build_compiled, or `hvm64 compile`) runs those
+ * functions instead of the instruction VM for that Book; any other Book runs
+ * on the VM as usual.  Buffer convention as hvm64_net_readback. */
+int hvm64_book_compile_source(const hvm64_book* book, char* buf, size_t cap, size_t* out_len);
+/* 1 when this library holds compiled functions for `book`'s Defs. */
+int hvm64_book_is_compiled(const hvm64_book* book);
 /* ast::Book::from_str + Display (ast/src/parser.rs, ast/src/ast.rs:221-232):
  * `book_text` as the reference prints a parsed Book.  References need not
  * resolve.  Buffer convention as hvm64_net_readback. */

@@ -199,6 +199,9 @@ std::unique_ptr<Emu> emu_reduce(const Book& book, uint32_t prog, unsigned thread
   E.P.labbits = reinterpret_cast<const ull*>(book.labbits.data());
   E.P.ndefs = unsigned(book.defs.size());
   E.P.ovf_flush = OVF_FLUSH;
+#ifdef HVM_GEN_INCLUDE
+  E.P.gen = book.defs.size() >= HVM_GEN_NDEFS && defs_hash(book, HVM_GEN_NDEFS) == HVM_GEN_HASH;
+#endif
   if (capture) {
     E.P.no_expand = 1;
     E.P.capture = capture->data();
@@ -367,4 +370,22 @@ extern "C" int hvm64emu_pre_reduce(const char* book_text, const char* skip, uint
     snprintf(err, errcap, "%s", e.what());
     return HVM64_ERR_BAD_INPUT;
   }
+}
+
+// 1 when this build carries compiled Def functions that match `book_text`
+// (a build with -DHVM_GEN_INCLUDE), else 0.
+extern "C" int hvm64emu_compiled_for(const char* book_text) {
+#ifdef HVM_GEN_INCLUDE
+  try {
+    Book book;
+    std::string src(book_text);
+    with_big_stack([&] { book.load(parse_book(src)); });
+    return book.defs.size() >= HVM_GEN_NDEFS && defs_hash(book, HVM_GEN_NDEFS) == HVM_GEN_HASH;
+  } catch (...) {
+    return 0;
+  }
+#else
+  (void)book_text;
+  return 0;
+#endif
 }

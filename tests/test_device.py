@@ -12,14 +12,15 @@ DEVICE_LIMIT = 50_000_000  # interactions; bigger fixtures get a 16 GiB heap and
 # rotations, label-heavy Church towers).  The GPU reduces them at the latency
 # of one chain of L2 round trips per interaction (about 0.1-1 M interactions/s),
 # so at full size they run for many minutes; they are checked on the CPU
-# emulation and at reduced sizes instead.
+# emulation and at reduced sizes instead.  (apelacion, 1.5·10^9 interactions,
+# is wide enough to run at about 13 M interactions/s: about two minutes.)
 SEQUENTIAL = {
     "tests::programs::stress_tests::sum_tail",
     "tests::programs::stress_tests::tuple_rots",
     "tests::programs::stress_tests::boom",
     "tests::programs::stress_tests::burn",
-    "tests::programs::stress_tests::apelacion",
 }
+LONG = {"tests::programs::stress_tests::apelacion"}  # given a 10-minute deadline
 
 
 def _hvm():
@@ -46,7 +47,7 @@ def test_device_snapshot(prog):
     1.4-1.5·10^9 interactions, Def calls that push about 60 redexes each)."""
     hvm64 = _hvm()
     big = prog["total"] > DEVICE_LIMIT
-    t = hvm64.Tuning(timeout_ms=300000 if big else 60000)
+    t = hvm64.Tuning(timeout_ms=600000 if prog["name"] in LONG else 300000 if big else 60000)
     text, rw = hvm64.run_book(prog["source"], heap_bytes=(16 << 30) if big else (1 << 30), tuning=t)
     assert text == prog["text"]
     assert rw == {k: prog[k] for k in ("anni", "comm", "eras", "dref", "oper")}
