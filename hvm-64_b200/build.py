@@ -95,6 +95,7 @@ def build_compiled(source, verbose=False):
         if verbose:
             sys.stderr.write(log)
         _run([NVCC, *ARCH, "-shared", "-o", lib, obj, os.path.join(OUT, "host.o"), "-lcudart"])
+        os.remove(obj)
     return lib
 
 

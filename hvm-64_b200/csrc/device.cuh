@@ -1238,6 +1238,95 @@ HVM_COLD unsigned gather_walk(unsigned net, ull root, ull* out, unsigned cap, ul
   return n;
 }
 
+// A normal form split for a parallel gather.  A single walk is a chain of
+// dependent loads, so one thread first expands the top of the tree breadth
+// first (at most GTOP words, until a level holds 32 items or more); the items
+// left at the edge, and every word that starts a redirect chain, become
+// subtrees that other threads walk with gather_walk.  Every subtree's pairs
+// form one contiguous run of gather_walk's depth-first order, so sizes summed
+// bottom-up over the expanded top give every run's offset.
+constexpr unsigned GTOP = 512, GTASKS = 256;
+enum : unsigned char { GATHER_LEAF = 0, GATHER_NODE = 1, GATHER_SUB = 2 };
+struct GatherTop {
+  ull* w;              // the item's word address
+  ull* v;              // its word (leaf and node items)
+  ull* sz;             // size in pairs, then (gather_place) offset
+  unsigned* ref;       // node: index of its first child (the second follows); subtree: its number
+  unsigned char* kind;
+  unsigned nt, nk;     // items, subtrees
+};
+HVM_DEV void gather_top(unsigned net, ull root, GatherTop& T) {
+  const ull hb = g_P.heap_bytes;
+  auto live = [&](ull p) {
+    ull a = p & A_MASK;
+    return (p >> 48) == 0 && a != 0 && a < hb;
+  };
+  unsigned nt = 1, nk = 0, lo = 0, hi = 1, depth = 0;
+  T.w[0] = root;
+  while (lo < hi) {
+    const unsigned width = hi - lo;
+    // (expanding a level adds at most `width` chain subtrees and 2 * width
+    // items to the next level, which may all become subtrees: checked here so
+    // that the numbers of items and subtrees stay within the arrays)
+    if (width >= 32u || nt + 2 * width > GTOP || nk + 3 * width > GTASKS || depth >= 48) {
+      for (unsigned k = lo; k < hi; k++) {  // the edge: subtrees
+        T.kind[k] = GATHER_SUB;
+        T.ref[k] = nk++;
+      }
+      break;
+    }
+    for (unsigned k = lo; k < hi; k++) {
+      ull v = ld_gpu(heap_at(net, T.w[k]));
+      T.v[k] = v;
+      unsigned t = unsigned(v & 7);
+      if (t == T_OP || t == T_CTR || t == T_SWITCH) {
+        T.kind[k] = GATHER_NODE;
+        T.ref[k] = nt;
+        T.w[nt++] = paddr(v);
+        T.w[nt++] = paddr(v) ^ 8;
+      } else if ((t == T_VAR || t == T_RED) && live(v)) {
+        T.kind[k] = GATHER_SUB;  // a redirect chain: walked as a subtree
+        T.ref[k] = nk++;
+      } else {
+        T.kind[k] = GATHER_LEAF;
+      }
+    }
+    lo = hi;
+    hi = nt;
+    depth++;
+  }
+  T.nt = nt;
+  T.nk = nk;
+}
+// Sizes bottom-up from the subtrees' counts (tc, by subtree number); returns
+// the whole walk's pair count.  (Children follow their parent in T.)
+HVM_DEV ull gather_sizes(GatherTop& T, const unsigned* tc) {
+  for (unsigned k = T.nt; k-- > 0;)
+    T.sz[k] = T.kind[k] == GATHER_LEAF ? 1
+              : T.kind[k] == GATHER_SUB ? ull(tc[T.ref[k]])
+                                        : 1 + T.sz[T.ref[k]] + T.sz[T.ref[k] + 1];
+  return T.sz[0];
+}
+// After gather_sizes: turns sizes into offsets (a node reads its first child's
+// size before overwriting it with the child's offset) and writes the top's
+// own words at theirs; the subtrees then go at T.sz[k].
+HVM_DEV void gather_place(GatherTop& T, const unsigned* tc, ull* dst) {
+  (void)tc;
+  T.sz[0] = 0;
+  for (unsigned k = 0; k < T.nt; k++) {
+    const ull at = T.sz[k];
+    if (T.kind[k] == GATHER_SUB) continue;
+    dst[2 * at] = T.w[k];
+    dst[2 * at + 1] = T.v[k];
+    if (T.kind[k] == GATHER_NODE) {
+      unsigned c = T.ref[k];
+      ull s0 = T.sz[c];
+      T.sz[c] = at + 1;
+      T.sz[c + 1] = at + 1 + s0;
+    }
+  }
+}
+
 #undef LS
 #undef FW
 

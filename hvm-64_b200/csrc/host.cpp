@@ -912,8 +912,52 @@ std::string compile_defs_cuda(const Book& book) {
     return std::string(buf);
   };
   auto r = [](unsigned i) { return "r" + std::to_string(i); };
+  // Which Defs get a function.  Long ones (literal data, such as an entry
+  // point holding a whole input tree, called once) stay on the VM.  A Book of
+  // many Defs (a batch: shared library Defs plus a few per net) compiles only
+  // the Defs reachable from two or more of its entry points (Defs no other Def
+  // references): compiling thousands of per-net Defs would take long and each
+  // runs for one net.
+  constexpr uint32_t MAX_INS = 128, ALL_BELOW = 512;
+  std::vector<std::vector<uint32_t>> refs(n);
+  std::vector<uint32_t> referrers(n, 0);
   for (uint32_t id = 0; id < n; id++) {
     const DevDef& d = book.defs[id];
+    for (uint32_t k = 0; k < d.ins_len; k++) {
+      const DevInstr& x = book.instrs[d.ins_off + k];
+      if ((x.k == I_CONST || x.k == I_LINKCONST) && (x.port & 7) == T_REF && !(x.port & EXPAND_BIT)) {
+        uint64_t t = ((x.port & ADDR_MASK) >> 3) - 1;
+        if (t < n && t != id) {
+          refs[id].push_back(uint32_t(t));
+          referrers[t]++;
+        }
+      }
+    }
+  }
+  std::vector<uint8_t> roots_reaching(n, 0);  // 0, 1 or 2 (two or more)
+  if (n > ALL_BELOW) {
+    std::vector<uint32_t> seen(n, ~0u), stack;
+    for (uint32_t root = 0; root < n; root++) {
+      if (referrers[root]) continue;
+      stack.assign(1, root);
+      seen[root] = root;
+      while (!stack.empty()) {
+        uint32_t v = stack.back();
+        stack.pop_back();
+        if (roots_reaching[v] < 2) roots_reaching[v]++;
+        for (uint32_t t : refs[v])
+          if (seen[t] != root) {
+            seen[t] = root;
+            stack.push_back(t);
+          }
+      }
+    }
+  }
+  std::vector<uint32_t> done;
+  for (uint32_t id = 0; id < n; id++) {
+    const DevDef& d = book.defs[id];
+    if (d.ins_len > MAX_INS || (n > ALL_BELOW && roots_reaching[id] < 2)) continue;
+    done.push_back(id);
     o += "// @" + book.names[id] + "\n";
     o += "HVM_COLD void gen_def_" + std::to_string(id) + "(const Ctx& c, ull r0) {\n";
     if (d.nregs > 1) {
@@ -949,7 +993,7 @@ std::string compile_defs_cuda(const Book& book) {
   }
   o += "\n// The Def's function for Def `id` (false: none; the VM runs it).\n";
   o += "HVM_INL bool gen_call(const Ctx& c, unsigned id, ull t0) {\n  switch (id) {\n";
-  for (uint32_t id = 0; id < n; id++)
+  for (uint32_t id : done)
     o += "    case " + std::to_string(id) + "u: gen_def_" + std::to_string(id) + "(c, t0); return true;\n";
   o += "  }\n  return false;\n}\n";
   return o;

@@ -220,22 +220,59 @@ __device__ __noinline__ unsigned serve_gather(WarpSmem& W, unsigned slot, ull ro
   return n < g_P.out_cap ? n : g_P.out_cap;
 }
 
-// Batch readback on the device: one thread per net counts (out == nullptr)
-// or writes its net's pairs at offs[i].  A net whose walk overflows the
-// stack gets count ~0u and is read back from a heap image instead.
+// Batch readback on the device: one warp per net counts its normal form's
+// (address, word) pairs (out == nullptr) or writes them at offs[i], in
+// gather_walk's order, with the net split into subtrees walked by the lanes
+// (gather_top, gather_sizes, gather_place).  The count pass keeps each
+// subtree's count in tcounts (GTASKS per net) for the write pass.  A net
+// whose walk overflows a lane's stack gets count ~0u and is read back from a
+// heap image instead.
 constexpr unsigned GATHER_STACK = 256;
-__global__ void gather_kernel(unsigned first, unsigned n, unsigned* counts, const ull* offs, ull* out) {
-  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  i += first;
+__global__ void __launch_bounds__(32) gather_kernel(unsigned first, unsigned n, unsigned* counts, const ull* offs,
+                                                    ull* out, unsigned* tcounts) {
+  __shared__ ull tw[GTOP], tv[GTOP], tsz[GTOP];
+  __shared__ unsigned tref[GTOP];
+  __shared__ unsigned char tkind[GTOP];
+  __shared__ unsigned ntop, bad;
+  const unsigned lane = threadIdx.x;
+  if (blockIdx.x >= n) return;
+  const unsigned i = first + blockIdx.x;
+  if (out && counts[i] == ~0u) return;
+  unsigned* tc = tcounts + size_t(blockIdx.x) * GTASKS;
+  GatherTop T{tw, tv, tsz, tref, tkind, 0, 0};
+  if (lane == 0) {
+    gather_top(i, g_P.nets[i].root, T);
+    ntop = T.nt;
+    bad = 0;
+  }
+  __syncwarp();
+  T.nt = ntop;
   ull stk[GATHER_STACK];
-  bool deep = false;
-  ull root = g_P.nets[i].root;
   if (!out) {
-    unsigned c = gather_walk(i, root, nullptr, 0, stk, GATHER_STACK, &deep);
-    counts[i] = deep ? ~0u : c;
-  } else if (counts[i] != ~0u) {
-    gather_walk(i, root, out + 2 * offs[i], counts[i], stk, GATHER_STACK, &deep);
+    for (unsigned k = lane; k < T.nt; k += 32) {
+      if (tkind[k] != GATHER_SUB) continue;
+      bool deep = false;
+      unsigned c = gather_walk(i, tw[k], nullptr, 0, stk, GATHER_STACK, &deep);
+      tc[tref[k]] = deep ? ~0u : c;
+      if (deep) bad = 1;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      ull total = gather_sizes(T, tc);
+      counts[i] = (bad || total >= 0xFFFFFFFFull) ? ~0u : unsigned(total);
+    }
+    return;
+  }
+  ull* dst = out + 2 * offs[i];
+  if (lane == 0) {
+    gather_sizes(T, tc);
+    gather_place(T, tc, dst);
+  }
+  __syncwarp();
+  for (unsigned k = lane; k < T.nt; k += 32) {
+    if (tkind[k] != GATHER_SUB) continue;
+    bool deep = false;
+    gather_walk(i, tw[k], dst + 2 * tsz[k], tc[tref[k]], stk, GATHER_STACK, &deep);
   }
 }
 
@@ -992,6 +1029,35 @@ void upload_params(const dev::Params& p, cudaStream_t st) {
 // bursts from Defs that create many redexes at once.
 constexpr unsigned DEFAULT_QLOG2 = 20;
 
+// Host staging for gathered normal forms, shared by the process's runs (one
+// gather at a time holds it).  Page-locked up to 4 GiB, so the copy from the
+// device runs at full link speed, and never zero-filled; it is kept for the
+// life of the process.
+struct HostStage {
+  std::mutex mu;
+  uint64_t* p = nullptr;
+  size_t bytes = 0;
+  bool pinned = false;
+  uint64_t* reserve(size_t need) {  // the caller holds mu
+    if (need <= bytes && p) return p;
+    if (p) {
+      if (pinned) cudaFreeHost(p);
+      else delete[] p;
+    }
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(need, size_t(64) << 20);
+    pinned = want <= (size_t(4) << 30) && cudaMallocHost(&p, want) == cudaSuccess;
+    if (!pinned) {
+      cudaGetLastError();  // a failed page-locked allocation is not an error of the run
+      p = new uint64_t[(want + 7) / 8];
+    }
+    bytes = want;
+    return p;
+  }
+};
+HostStage g_stage;
+
 // A set of nets reduced together on the current device.
 struct Runner {
   Book book;
@@ -1378,9 +1444,10 @@ struct Runner {
   // (address, word) pairs; a count of ~0u sends that net to the heap image.
   bool pairs_valid = false;
   std::vector<unsigned> gcount;
-  std::vector<uint64_t> goff, gpairs;
+  std::vector<uint64_t> goff;
   DevBuf<unsigned> d_gcount;
   DevBuf<dev::ull> d_goff, d_gpairs;
+  DevBuf<unsigned> d_tcounts;  // gather_kernel's per-subtree counts
 
   // Gathers the normal forms of the last run's nets (device-side walk).
   void gather_all() {
@@ -1388,13 +1455,11 @@ struct Runner {
     DeviceTurn turn(device, 600000);
     upload_params(params(), 0);
     d_gcount.alloc(n);
-    // one thread per net; small blocks spread the (latency-bound) walks over
-    // as many SMs as there are warps of nets
-    constexpr unsigned GB = 32;
-    unsigned blocks = (cnt + GB - 1) / GB;
+    // one warp per net (see gather_kernel)
     gcount.assign(n, ~0u);
+    d_tcounts.alloc(size_t(std::max(cnt, 1u)) * dev::GTASKS);
     if (cnt) CU(cudaMemcpy(d_gcount.p, gcount.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
-    if (cnt) dev::gather_kernel<<<blocks, GB>>>(first, cnt, d_gcount.p, nullptr, nullptr);
+    if (cnt) dev::gather_kernel<<<cnt, 32>>>(first, cnt, d_gcount.p, nullptr, nullptr, d_tcounts.p);
     CU(cudaGetLastError());
     CU(cudaMemcpy(gcount.data(), d_gcount.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     for (unsigned i = 0; i < n; i++)
@@ -1408,17 +1473,18 @@ struct Runner {
     d_goff.alloc(n);
     CU(cudaMemcpy(d_goff.p, goff.data(), size_t(n) * 8, cudaMemcpyHostToDevice));
     d_gpairs.alloc(2 * tot);
-    if (cnt) dev::gather_kernel<<<blocks, GB>>>(first, cnt, d_gcount.p, d_goff.p, d_gpairs.p);
+    if (cnt) dev::gather_kernel<<<cnt, 32>>>(first, cnt, d_gcount.p, d_goff.p, d_gpairs.p, d_tcounts.p);
     CU(cudaGetLastError());
-    gpairs.resize(2 * tot);
-    if (tot) CU(cudaMemcpy(gpairs.data(), d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
+    std::lock_guard<std::mutex> staged(g_stage.mu);
+    uint64_t* pairs = g_stage.reserve(16 * tot);
+    if (tot) CU(cudaMemcpy(pairs, d_gpairs.p, 16 * tot, cudaMemcpyDeviceToHost));
     d2h += size_t(n) * 4 + 16 * tot;
     h2d += size_t(n) * 8;
     // Every gathered net's text at once, on the host's cores.
     std::vector<uint64_t> roots(cnt);
     for (unsigned i = 0; i < cnt; i++) roots[i] = host_nets[first + i].root;
     unsigned hw = std::thread::hardware_concurrency();
-    gtext = readback_pairs_many(book, gpairs.data(), goff.data() + first, gcount.data() + first, roots.data(), cnt,
+    gtext = readback_pairs_many(book, pairs, goff.data() + first, gcount.data() + first, roots.data(), cnt,
                                 heap_bytes / 8, std::max(1u, std::min(hw ? hw : 1u, 16u)));
     pairs_valid = true;
   }

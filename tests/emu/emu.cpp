@@ -272,6 +272,30 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
         n = gather_walk(0, E.nets[0].root, pairs.data(), n, stk.data(), 256, &deep);
       }
       if (!deep) {
+        // The batch gather's split walk (the top expanded by one thread, the
+        // subtrees walked separately) must give the same pairs in the same order.
+        {
+          std::vector<ull> tw(GTOP), tv(GTOP), tsz(GTOP), sp(256);
+          std::vector<unsigned> tref(GTOP), tc(GTASKS);
+          std::vector<unsigned char> tkind(GTOP);
+          GatherTop T{tw.data(), tv.data(), tsz.data(), tref.data(), tkind.data(), 0, 0};
+          gather_top(0, E.nets[0].root, T);
+          bool sdeep = false;
+          for (unsigned k = 0; k < T.nt; k++)
+            if (tkind[k] == GATHER_SUB) tc[tref[k]] = gather_walk(0, tw[k], nullptr, 0, sp.data(), 256, &sdeep);
+          ull total = gather_sizes(T, tc.data());
+          if (!sdeep) {
+            if (total != n) throw Error(HVM64_ERR_BAD_INPUT, "split gather counts " + std::to_string(total) +
+                                                                 " pairs, the walk " + std::to_string(n));
+            std::vector<ull> split(2 * size_t(n) + 2, 0);
+            gather_place(T, tc.data(), split.data());
+            for (unsigned k = 0; k < T.nt; k++)
+              if (tkind[k] == GATHER_SUB)
+                gather_walk(0, tw[k], split.data() + 2 * tsz[k], tc[tref[k]], sp.data(), 256, &sdeep);
+            for (size_t k = 0; k < 2 * size_t(n); k++)
+              if (split[k] != pairs[k]) throw Error(HVM64_ERR_BAD_INPUT, "split gather differs at " + std::to_string(k));
+          }
+        }
         std::string g;
         with_big_stack([&] { g = readback_pairs(book, reinterpret_cast<const uint64_t*>(pairs.data()), n,
                                                 E.heap.size(), E.nets[0].root); });
