@@ -1033,9 +1033,10 @@ struct PreReduceDfs {
     seen[name] = 1;
     if (r.status && r.status != HVM64_ERR_LIMIT)
       throw Error(r.status, "pre-reducing @" + name + ": " + r.error);
-    // Net::reduce(limit) reports normal form when fewer than `limit` redexes
-    // were popped (net.rs:41-52).
-    if (r.status == HVM64_ERR_LIMIT || r.pops >= max_rwts) {
+    // Net::reduce(limit) stops, reporting no normal form, once it has popped
+    // `limit` redexes; it checks after each pop, so a reduction that pops
+    // none is normal whatever the limit (net.rs:41-52).
+    if (r.status == HVM64_ERR_LIMIT || (r.pops > 0 && r.pops >= max_rwts)) {
       // The reference keeps the net as it stood after max_rwts pops; a device
       // run does not stop at an exact pop, so the Def keeps its original net
       // (and adds no Rewrites).  Either way it is reported as not normal.

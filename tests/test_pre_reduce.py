@@ -163,11 +163,23 @@ def test_emu_fast_pre_reduce(case):
 @pytest.mark.parametrize("limit", [10, 50, 400, 5000])
 def test_emu_rewrite_limit_lists_the_oracles_defs(limit):
     """A Def whose reduction pops `limit` redexes or more is not normal in
-    both; the device keeps its original net."""
+    both; the device keeps its original net.  (The lists agree while no Def
+    that stopped short is called by one reduced after it: the reference's
+    later Defs then call the partly reduced net, the device's the original.)"""
     src = next(p for p in PRE if p["name"] == "tests::programs::dec_bits_tree")["source"]
     _, _, want = oracle.pre_reduce(src, skip=("main",), max_rwts=limit)
     _, _, got = emu_pre_reduce(src, max_rwts=limit)
     assert got == want
+
+
+def test_emu_limit_zero_leaves_defs_without_redexes_normal():
+    """Net::reduce(0) pops once before it checks the limit, so a Def with no
+    redex after its boot is normal under any limit (net.rs:41-52)."""
+    src = "@add = ($([+] $(a b)) (a b))\n@main = a & @add ~ (1 (2 a))\n@two = a & @add ~ (1 (1 a))"
+    for limit in (0, 1):
+        want_text, want_rw, want = oracle.pre_reduce(src, skip=("main",), max_rwts=limit)
+        text, rw, got = emu_pre_reduce(src, max_rwts=limit)
+        assert want == got == ["two"]
 
 
 # ---- on the GPU --------------------------------------------------------------------
