@@ -276,36 +276,37 @@ def serve_leg(args, hvm64):
         life_ms = int(1000 * (arr[-1] + args.serve_wait_s)) + 5000
         sv = hvm64.Server(book, slots=args.serve_slots, out_pairs=1 << 19, heap_bytes=16 << 30,
                           tuning=hvm64.Tuning(timeout_ms=life_ms))
-        lat, owner, i, texts = [], {}, 0, []
-        t_start = time.perf_counter()
-        last = 0.0
-        while len(lat) < len(names):
-            now = time.perf_counter() - t_start
-            if now > arr[-1] + args.serve_wait_s:
-                sv.close()
-                raise RuntimeError(f"serving: {len(names) - len(lat)} requests unfinished "
-                                   f"{args.serve_wait_s} s after the last arrival")
-            busy = False
-            while i < len(names) and arr[i] <= now:
-                try:
-                    owner[sv.submit(names[i], nodes=nodes[i])] = i
-                except hvm64.HvmError as e:  # no slot or node budget free: admit later
-                    if e.code != hvm64.ERR_QUEUE:
-                        raise
-                    break
-                i += 1
-                busy = True
-            for tk in sv.poll():
-                k = owner.pop(tk)
-                text, rw, us = sv.result(tk)
-                last = time.perf_counter() - t_start
-                lat.append(last - arr[k])
-                texts.append((k, text))
-                busy = True
-            if not busy:
-                time.sleep(0.0002)
-        heap = sv.budget()
-        sv.close()
+        try:
+            lat, owner, i, texts = [], {}, 0, []
+            t_start = time.perf_counter()
+            last = 0.0
+            while len(lat) < len(names):
+                now = time.perf_counter() - t_start
+                if now > arr[-1] + args.serve_wait_s:
+                    raise RuntimeError(f"serving: {len(names) - len(lat)} requests unfinished "
+                                       f"{args.serve_wait_s} s after the last arrival")
+                busy = False
+                while i < len(names) and arr[i] <= now:
+                    try:
+                        owner[sv.submit(names[i], nodes=nodes[i])] = i
+                    except hvm64.HvmError as e:  # no slot or node budget free: admit later
+                        if e.code != hvm64.ERR_QUEUE:
+                            raise
+                        break
+                    i += 1
+                    busy = True
+                for tk in sv.poll():
+                    k = owner.pop(tk)
+                    text, rw, us = sv.result(tk)
+                    last = time.perf_counter() - t_start
+                    lat.append(last - arr[k])
+                    texts.append((k, text))
+                    busy = True
+                if not busy:
+                    time.sleep(0.0002)
+            heap = sv.budget()
+        finally:  # a failed load still frees its server (and the device it holds)
+            sv.close()
         bad += sum(0 if W.check_request(*reqs[k], text) else 1 for k, text in texts)
         loads.append({
             "offered_rps": rate, "offered_frac_of_plain_capacity": frac,
