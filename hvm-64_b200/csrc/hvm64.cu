@@ -1682,10 +1682,13 @@ struct Server {
     c.heap_nodes = heap_bytes / 16;
     c.heap_bytes = heap_bytes;
     // small allocator chunks: a server's heap is shared by requests for its
-    // whole life, so nodes stranded in part-used chunks count against it; and
-    // free nodes are shared between warps from the start
+    // whole life, so nodes stranded in part-used chunks count against it.
+    // Free nodes are shared between warps once half the heap is used, as in a
+    // batch run: sharing them from the start measured 3-5x longer tail
+    // latencies (allocation from shared lists is a chain of dependent loads)
+    // and, in some runs, a stalled reducer.
     c.chunk_nodes = t.chunk_nodes ? t.chunk_nodes : 32;
-    c.reuse_mark = 0;
+    c.reuse_mark = c.heap_nodes / 2;
     c.spin_limit = 1ull << 24;
     c.donate_min = t.donate_min ? t.donate_min : 64;
     c.max_warps = t.max_warps_per_net;

@@ -197,8 +197,9 @@ int hvm64_server_submit(hvm64_server* server, const char* def_name, uint64_t* ti
  * lists, per-warp pools); a request is admitted when a slot and `nodes` of the
  * budget are free (else HVM64_ERR_QUEUE: collect results and retry), and its
  * reservation returns with its result.  Nodes a finished request's normal
- * form used are recycled for later requests, so a long-running server's heap
- * stays bounded by what its requests hold at once. */
+ * form used are recycled for later requests; once half the heap is in use,
+ * free nodes also move between the reducer's warps, so a long-running
+ * server's heap stops growing at about half its size. */
 int hvm64_server_submit_nodes(hvm64_server* server, const char* def_name, uint64_t nodes, uint64_t* ticket);
 /* The node budget, the part admitted requests hold, and the heap's high-water
  * mark (nodes ever taken from fresh memory). */

@@ -122,14 +122,15 @@ def test_server_long_run_heap_stays_bounded():
     """600 bitonic-sort requests (2^12 keys each; about 12,000 nodes of
     normal form per request) through one server, 32 at a time, each admitted
     against the node budget: every result is right, the reservation returns
-    to zero, and once the allocator's per-lane reserve has filled (the first
-    half of the run) the heap's high-water mark stops growing: the last 300
-    requests add far less than the 3.6 million nodes their normal forms alone
-    would hold if finished requests' nodes were not recycled."""
+    to zero, and once half the heap is in use (the point from which free
+    nodes move between warps; a 1 GiB heap reaches it in the first half of
+    the run) the heap's high-water mark stops growing: the last 300 requests
+    add far less than the 3.6 million nodes their normal forms alone would
+    hold if finished requests' nodes were not recycled."""
     hvm64 = _hvm()
     reqs = [("sort", 12, j) for j in range(8)]
     book = hvm64.Book.from_str(W.serving_book(reqs))
-    sv = hvm64.Server(book, slots=32, out_pairs=1 << 18, heap_bytes=4 << 30,
+    sv = hvm64.Server(book, slots=32, out_pairs=1 << 18, heap_bytes=1 << 30,
                       tuning=hvm64.Tuning(timeout_ms=300000))
     try:
         owner, done, submitted, high = {}, 0, 0, {}
