@@ -299,6 +299,18 @@ inline void lock_fill(ull* H, ull s, ull n) {
   for (ull k = 0; k < 2 * n; k++) st_gpu(H + 2 * s + k, P_LOCK);
 }
 #endif
+#ifdef HVM_EMU_CHECK_ALLOC
+// Host test builds only: per node, whether it is handed out (top bit); a node
+// handed out while out, or reclaimed while not out, is counted here.
+inline std::atomic<unsigned>* g_node_out = nullptr;
+inline std::atomic<unsigned long long> g_alloc_faults{0};
+inline void check_handed_out(ull node) {
+  if (node && (g_node_out[node >> 4].fetch_or(1u) & 1u)) g_alloc_faults++;
+}
+inline void check_reclaimed(ull node) {
+  if (!(g_node_out[node >> 4].fetch_and(~1u) & 1u)) g_alloc_faults++;
+}
+#endif
 HVM_INL long long ld_gpu64s(const long long* p) {
   return (long long)ld_gpu(reinterpret_cast<const ull*>(p));
 }
@@ -589,6 +601,9 @@ HVM_INL ull lock_target(const Ctx& c, ull w) {
 // without reading the other half; otherwise the reference's store-FREE /
 // read-other-half / CAS sequence decides which lane reclaims.
 HVM_COLD void recycle(const Ctx& c, ull node) {
+#ifdef HVM_EMU_CHECK_ALLOC
+  check_reclaimed(node);
+#endif
   int k = c.W->pool_cap ? smem_add_i32(&c.W->freed_n, 1) : POOL;
   if (k < c.W->pool_cap) {
     c.W->freed[k] = node;
@@ -604,7 +619,17 @@ HVM_COLD ull alloc_slow(const Ctx& c) {
   }
   return r.node;
 }
+#ifdef HVM_EMU_CHECK_ALLOC
+HVM_INL ull alloc_unchecked(const Ctx& c);
 HVM_INL ull alloc(const Ctx& c) {
+  ull n = alloc_unchecked(c);
+  check_handed_out(n);
+  return n;
+}
+HVM_INL ull alloc_unchecked(const Ctx& c) {
+#else
+HVM_INL ull alloc(const Ctx& c) {
+#endif
   LS(allocs)++;
   if (c.W->pool_cap) {
     int k = smem_add_i32(&c.W->pool_n, -1) - 1;

@@ -179,6 +179,12 @@ std::unique_ptr<Emu> emu_reduce(const Book& book, uint32_t prog, unsigned thread
                                 std::vector<ull>* capture) {
   auto Ep = std::make_unique<Emu>();
   Emu& E = *Ep;
+#ifdef HVM_EMU_CHECK_ALLOC
+  static std::vector<std::atomic<unsigned>> node_out;
+  node_out = std::vector<std::atomic<unsigned>>(heap_bytes / 16);
+  g_node_out = node_out.data();
+  g_alloc_faults = 0;
+#endif
   E.heap.assign(heap_bytes / 8, 0);
   E.nets.assign(1, NetState{});
   E.nets[0].prog = int(prog);
@@ -258,6 +264,13 @@ extern "C" int hvm64emu_run(const char* book_text, const char* entry, unsigned t
       snprintf(err, errcap, "device error %d info 0x%llx", E.C.error, (unsigned long long)E.C.error_info);
       return E.C.error;
     }
+#ifdef HVM_EMU_CHECK_ALLOC
+    if (g_alloc_faults.load()) {
+      snprintf(err, errcap, "%llu nodes handed out twice or reclaimed twice",
+               (unsigned long long)g_alloc_faults.load());
+      return HVM64_ERR_BAD_ADDR;
+    }
+#endif
     for (int k = 0; k < 5; k++) rw[k] = E.nets[0].rw[k];
     std::string txt;
     with_big_stack([&] { txt = readback(book, reinterpret_cast<const uint64_t*>(E.heap.data()), E.heap.size(), E.nets[0].root); });

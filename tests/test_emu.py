@@ -112,3 +112,39 @@ def test_emu_def_with_many_live_wires():
     text, rw = emu_run(src, threads=4)
     assert text == want
     assert rw == want_rw
+
+
+CHECK_SO = os.path.join(HERE, "emu", "build", "libhvm64_emu_check.so")
+
+
+def _check_lib():
+    """The emulation built with allocator bookkeeping (HVM_EMU_CHECK_ALLOC):
+    every node handed out is marked, and handing out a marked node or
+    reclaiming an unmarked one is counted and fails the run."""
+    if not os.path.exists(CHECK_SO) or any(os.path.getmtime(d) > os.path.getmtime(CHECK_SO) for d in DEPS):
+        os.makedirs(os.path.dirname(CHECK_SO), exist_ok=True)
+        subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", "-DHVM_EMU_STRESS",
+                        "-DHVM_OVF_FLUSH=4", "-DHVM_EMU_CHECK_ALLOC",
+                        "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "hvm-64_b200", "csrc"),
+                        *SRC, "-o", CHECK_SO], check=True)
+    L = ctypes.CDLL(CHECK_SO)
+    c = ctypes
+    L.hvm64emu_run.argtypes = [c.c_char_p, c.c_char_p, c.c_uint, c.c_uint, c.c_uint, c.c_uint, c.c_uint64,
+                               c.c_uint64, c.POINTER(c.c_char_p), c.POINTER(c.c_uint64), c.c_char_p, c.c_size_t]
+    return L
+
+
+@pytest.mark.parametrize("prog", [p for p in PROGRAMS if p["total"] <= 3_000_000], ids=lambda p: p["name"])
+def test_emu_never_hands_out_a_node_twice(prog):
+    """Under jittered contention (16 host threads, free lists published to
+    the shared stack after 4 nodes, half the lanes without a reuse pool), no
+    node is handed out while already out and none is reclaimed twice: the
+    free / claim / recycle protocol and the shared free stack keep each node
+    with one owner at a time."""
+    L = _check_lib()
+    out = ctypes.c_char_p()
+    rw = (ctypes.c_uint64 * 5)()
+    err = ctypes.create_string_buffer(256)
+    rc = L.hvm64emu_run(prog["source"].encode(), b"main", 16, 2, 24, 16, 1 << 30, 32, ctypes.byref(out), rw, err, 256)
+    assert rc == 0, err.value.decode()
+    assert out.value.decode() == prog["text"]
